@@ -1,0 +1,142 @@
+/*
+ * ref_driver.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A thin extern "C" driver over the reference's own CJMultiSlice class
+ * (src/JMultiSlice.h:185-738), compiled together with the reference sources
+ * by oracle/Makefile into oracle/_ref/libjms_ref.so.  Tests use it to make
+ * golden vectors and to check the FP64 oracle; bench.py's reference arm uses
+ * it to time the reference CPU path (CPUMultislice on MKL DFTI).  Nothing in
+ * the product links or loads this file.
+ *
+ * Every function forwards to the reference method of the same name; no
+ * reference source is copied here.
+ */
+#include "JMultiSlice.h"
+#include <atomic>
+#include <thread>
+#include <vector>
+#include <string>
+#include <cstring>
+
+// Exposes protected reference methods needed for golden vectors.
+class RefJMS : public CJMultiSlice {
+public:
+	using CJMultiSlice::GetRandomVariantSequence; // JMultiSlice.cpp:1571
+	fcmplx* cpu_wave(int ithread) { // thread wave slot after OffsetIncomingWave (JMultiSlice.cpp:2024)
+		return m_h_wav + (int64_t)m_nscx * m_nscy * ithread;
+	}
+};
+
+extern "C" {
+
+void* ref_create(void) { return new RefJMS(); }
+void ref_destroy(void* h) { delete (RefJMS*)h; }
+
+float ref_set_high_tension(void* h, float ht) { ((RefJMS*)h)->SetHighTension(ht); return ((RefJMS*)h)->GetWaveLength(); }
+void ref_set_grid(void* h, int nx, int ny, float a, float b, float c)
+{
+	((RefJMS*)h)->SetGridSize(nx, ny);
+	((RefJMS*)h)->SetSupercellSize(a, b, c);
+}
+void ref_seed(void* h, int seed) { ((RefJMS*)h)->SeedRngEx(seed); }
+
+int ref_phase_grating_setup(void* h, int code, int nx, int ny, int nslc, int nvarmax, int* nslcvar)
+{ return ((RefJMS*)h)->PhaseGratingSetup(code, nx, ny, nslc, nvarmax, nslcvar); }
+int ref_object_slice_setup(void* h, int nobjslc, int* objslc)
+{ return ((RefJMS*)h)->ObjectSliceSetup(nobjslc, objslc); }
+int ref_propagator_setup(void* h, int code, int npro, int* proidx)
+{ return ((RefJMS*)h)->PropagatorSetup(code, npro, proidx); }
+int ref_detector_setup(void* h, int code, int ndetper, int ndetint, int imagedet, int nthreads)
+{ return ((RefJMS*)h)->DetectorSetup(code, ndetper, ndetint, imagedet, nthreads); }
+int ref_set_phase_grating(void* h, int code, int islc, int nvar, float* pgr)
+{ return ((RefJMS*)h)->SetPhaseGratingData(code, islc, nvar, (fcmplx*)pgr); }
+int ref_set_propagator(void* h, int code, int ipro, float* pro)
+{ return ((RefJMS*)h)->SetPropagatorData(code, ipro, (fcmplx*)pro); }
+int ref_set_detector(void* h, int code, int idet, float* det, int msklen, int* msk)
+{ return ((RefJMS*)h)->SetDetectorData(code, idet, det, msklen, msk); }
+int ref_init_core(void* h, int code, int nthreads) { return ((RefJMS*)h)->InitCore(code, nthreads); }
+int ref_set_incident_wave(void* h, int code, float* wav) { return ((RefJMS*)h)->SetIncidentWave(code, (fcmplx*)wav); }
+int ref_set_phaseplate(void* h, int code, float* ppl) { return ((RefJMS*)h)->SetIncidentWavePhaseplate(code, ppl); }
+int ref_offset_incoming_wave(void* h, int code, float dx, float dy, float dz, int ithread, int ibtx, int ibty)
+{ return ((RefJMS*)h)->OffsetIncomingWave(code, dx, dy, dz, ithread, ibtx, ibty); }
+int ref_cpu_multislice(void* h, int islc0, int accmode, float weight, int ithread)
+{ return ((RefJMS*)h)->CPUMultislice(islc0, accmode, weight, ithread); }
+int ref_gpu_multislice(void* h, int islc0, int accmode, float weight)
+{ return ((RefJMS*)h)->GPUMultislice(islc0, accmode, weight); }
+int ref_get_result(void* h, int code, int which, float* dst, int ithread)
+{ return ((RefJMS*)h)->GetResult(code, which, dst, ithread); }
+int ref_get_avg_result(void* h, int code, int which, float* dst, float* wgt, int ithread)
+{ float w = 0.f; int e = ((RefJMS*)h)->GetAvgResult(code, which, dst, w, ithread); *wgt = w; return e; }
+int ref_num_det_planes(void* h) { return ((RefJMS*)h)->GetDetetionSliceNum(); }
+int ref_unscramble_hash(void* h, unsigned int* hash) { return ((RefJMS*)h)->GetUnscrambleHash(hash); }
+int ref_variant_sequence(void* h, int* out) { return ((RefJMS*)h)->GetRandomVariantSequence(out); }
+void ref_cpu_wave(void* h, int ithread, float* dst, int n)
+{ memcpy(dst, ((RefJMS*)h)->cpu_wave(ithread), sizeof(fcmplx) * (size_t)n); }
+int ref_detection_planes(void* h, int ndetper, int nobjslc, int* det_objslc)
+{ return ((RefJMS*)h)->SetDetectionPlanes(ndetper, nobjslc, det_objslc); }
+int ref_cleanup(void* h) { return ((RefJMS*)h)->Cleanup(); }
+
+// CalculateProbeWaveFourier (JMultiSlice.cpp:983) with the public CJProbeParams
+// fields (JProbeGen.h:60-94); abrr holds 2*24 coefficients [nm].
+int ref_calc_probe(void* h, float alpha, float alpha_rs, float alpha_x0, float alpha_y0,
+	float alpha_asym, float alpha_adir, float btx, float bty, const float* abrr, int nabrr2, float* wav)
+{
+	CJProbeParams prm;
+	prm.m_alpha = alpha; prm.m_alpha_rs = alpha_rs;
+	prm.m_alpha_x0 = alpha_x0; prm.m_alpha_y0 = alpha_y0;
+	prm.m_alpha_asym = alpha_asym; prm.m_alpha_adir = alpha_adir;
+	prm.m_btx = btx; prm.m_bty = bty;
+	int nac = 2 * prm.GetAberrationNum();
+	for (int i = 0; i < nac && i < nabrr2; i++) prm.m_abrr_coeff[i] = abrr[i];
+	return ((RefJMS*)h)->CalculateProbeWaveFourier(&prm, (fcmplx*)wav);
+}
+int ref_calc_propagator(void* h, float fthick, float otx, float oty, int ntype, float* pro)
+{ return ((RefJMS*)h)->CalculatePropagator(fthick, otx, oty, (fcmplx*)pro, ntype); }
+int ref_calc_ring_detector(void* h, float beta0, float beta1, float phi0, float phi1,
+	float th0x, float th0y, const char* profile, float* det, int* msklen, int* msk, int kmom1)
+{
+	int ml = 0;
+	int e = ((RefJMS*)h)->CalculateRingDetector(beta0, beta1, phi0, phi1, th0x, th0y,
+		std::string(profile ? profile : ""), det, ml, msk, kmom1);
+	*msklen = ml;
+	return e;
+}
+
+// Multi-threaded reference CPU scan, following the hybrid queue of the
+// reference benchmark (test/JMSBench1/multislice.cpp:1236-1416): worker
+// threads pull probe positions from a shared counter; per position they run
+// nrepeat frozen-phonon passes of OffsetIncomingWave + CPUMultislice with
+// weight 1/nrepeat and read the integrated detectors.  Each worker owns one
+// CJMultiSlice object (the CPU path borrows the caller's host arrays, so the
+// objects share gratings, propagators and detectors) and runs MKL
+// sequentially, as the reference links mkl_sequential.
+// objs: nthreads handles, each fully set up for CPU code with 1 thread channel.
+// pos: npos (dx,dy) pairs [nm]; out: npos * ndetslc * ndet floats.
+int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrepeat,
+	int ndetout, float* out)
+{
+	std::atomic<int> next(0);
+	std::atomic<int> err(0);
+	std::vector<std::thread> pool;
+	for (int t = 0; t < nthreads; t++) {
+		pool.emplace_back([&, t]() {
+			mkl_set_num_threads_local(1);
+			RefJMS* jms = (RefJMS*)objs[t];
+			float w = 1.f / (float)nrepeat;
+			for (;;) {
+				int ip = next.fetch_add(1);
+				if (ip >= npos) break;
+				for (int ir = 0; ir < nrepeat; ir++) {
+					int e = jms->OffsetIncomingWave(_JMS_CODE_CPU, pos[2 * ip], pos[2 * ip + 1], 0.f, 0);
+					if (e == 0) e = jms->CPUMultislice(0, ir > 0 ? 1 : 0, w, 0);
+					if (e != 0) { err.store(e); return; }
+				}
+				jms->GetResult(_JMS_CODE_CPU, _JMS_DETECT_INTEGRATED, out + (size_t)ip * ndetout, 0);
+			}
+		});
+	}
+	for (auto& th : pool) th.join();
+	return err.load();
+}
+
+} // extern "C"
