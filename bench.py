@@ -1,0 +1,409 @@
+"""Benchmark of the multislice hot path: multislice steps/s on 512^2 waves.
+
+Workload (one line of the headline STEM scan, see jmultislicelib_b200/synthetic.py
+SCAN_512): 512x512 complex64 waves, 200 slices over 4 slice types with 16
+frozen-phonon variants each, 300 kV / 22 mrad / Cs 1 um probe, Fresnel
+propagator with 2/3 band limit, 3 annular detectors read every 20 slices plus
+the 128x128 binned exit diffraction pattern.  One bench step = one raster row
+of 64 probe positions x 16 phonon passes x 200 slices = 204,800 multislice
+steps (the full scan is 64 such rows).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed.run, one rank per GPU; each rank takes its
+own raster rows (weak scaling, no data-path collective); timing is the max
+over ranks.  --impl reference times the reference's own CPU path
+(CJMultiSlice::CPUMultislice on MKL, compiled from the reference sources into
+oracle/_ref) on the host cores with the same workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "multislice steps/s (512² wave)"
+UNIT = "steps/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref): the reported baseline and the reference arm
+# ---------------------------------------------------------------------------
+def reference_cpu(cfg, sp, probe, pro, dets, pos, nthreads, npos_sample, npass_sample=1):
+    """Times CJMultiSlice::CPUMultislice of the reference on nthreads host
+    threads over npos_sample positions x npass_sample passes; returns steps/s."""
+    from oracle import ref
+
+    if not ref.available():
+        raise RuntimeError("oracle/_ref/libjms_ref.so is not built")
+    objs = []
+    objslc = np.arange(cfg["nobj"]) % cfg["nslice_types"]
+    for t in range(nthreads):
+        R = ref.RefJMS()
+        R.set_high_tension(cfg["kv"])
+        R.set_grid(cfg["nx"], cfg["ny"], sp.a, sp.b, 0.19525)
+        R.setup(ref.CODE_CPU, [cfg["nvar"]] * cfg["nslice_types"], objslc, [0] * cfg["nslice_types"],
+                cfg["ndetper"], len(dets), 1, 1)
+        for s, gr in enumerate(sp.gratings):
+            R.set_phase_grating(ref.CODE_CPU, s, gr)
+        R.set_propagator(ref.CODE_CPU, 0, pro)
+        for i, (d, m) in enumerate(dets):
+            R.set_detector(ref.CODE_CPU, i, d, m)
+        R.init_core(ref.CODE_CPU, 1)
+        R.set_incident_wave(ref.CODE_CPU, probe)
+        R.seed(1000 + t)
+        objs.append(R)
+    nd = objs[0].num_det_planes()
+    sample = pos[:npos_sample]
+    t0 = time.perf_counter()
+    out, e = ref.cpu_scan(objs, sample, npass_sample, nd * len(dets))
+    dt = time.perf_counter() - t0
+    assert e == 0, e
+    for R in objs:
+        R.close()
+    steps = npos_sample * npass_sample * cfg["nobj"]
+    return steps / dt, dt, out
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from jmultislicelib_b200 import synthetic as S
+
+    cfg = S.SCAN_512
+    try:
+        from oracle import ref
+        if not ref.available():
+            raise RuntimeError("reference library oracle/_ref/libjms_ref.so missing")
+    except Exception as ex:
+        print(json.dumps({"impl": "reference", "unavailable": str(ex)}))
+        return 0
+    sp = S.make_specimen(cfg["nx"], cfg["ny"], cfg["ncell"], cfg["ncell"], cfg["nslice_types"], cfg["nvar"],
+                         cfg["seed"], cfg["kv"])
+    # the reference's own generators provide probe, propagator and detectors
+    R = ref.RefJMS()
+    R.set_high_tension(cfg["kv"])
+    R.set_grid(cfg["nx"], cfg["ny"], sp.a, sp.b, 0.19525)
+    pro = R.calc_propagator(0.19525, 0.0, 0.0, cfg["ntype"])
+    dets = [R.calc_ring_detector(b0, b1) for (b0, b1) in cfg["dets"]]
+    ab = np.zeros(48, np.float32)
+    ab[10] = cfg["cs"]
+    probe = R.calc_probe(cfg["alpha"], abrr=ab)
+    R.close()
+    mid = (cfg["ncell"] // 2) * S.A_CELL
+    pos = S.scan_positions(cfg["nscan"], mid, mid, S.A_CELL)
+    nt = host_threads()
+    per_step = nt  # one position-pass per thread per step
+    rates, times = [], []
+    for it in range(args.warmup + args.steps):
+        sel = pos[(it * per_step) % len(pos):][:per_step]
+        if len(sel) < per_step:
+            sel = pos[:per_step]
+        r, dt, _ = reference_cpu(cfg, sp, probe, pro, dets, sel, nt, per_step)
+        if it >= args.warmup:
+            rates.append(r)
+            times.append(dt)
+    value = per_step * cfg["nobj"] * len(times) / sum(times)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "STEM scan 512^2, 200 slices, 4 slice types x 16 phonon variants; "
+                                   f"bench step = {per_step} position-passes on the host threads",
+                       "grid": 512, "slices": cfg["nobj"]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "reference",
+                             "sample": f"{per_step} probe positions x 1 phonon pass x 200 slices per step "
+                                       "(CJMultiSlice::CPUMultislice on MKL DFTI, one thread per position)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# product arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    import jmultislicelib_b200 as jb
+    from jmultislicelib_b200 import synthetic as S
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg = S.SCAN_512
+    J = jb.JMS()
+    J.L.SetCurrentGPU(local)
+    stream = torch.cuda.Stream()
+    J.set_stream(stream.cuda_stream)
+    J.L.JMS_SetScanBatch(args.batch)
+    sp, probe, pro, dets, pos = S.setup_library(J, cfg)
+    J.seed(4242 + rank)
+    nd = J.num_det_planes()
+    ndet = len(dets)
+    npos_step = cfg["nscan"]            # one raster row
+    npass = cfg["nvar"]
+    bin_ = cfg["bin"]
+    nbx, nby = cfg["nx"] // bin_, cfg["ny"] // bin_
+    steps_per_bench_step = npos_step * npass * cfg["nobj"]
+    dev = torch.device("cuda", local)
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_int = torch.zeros((len(pos), nd, ndet), dtype=torch.float64, device=dev)
+    d_bin = torch.zeros((npos_step, nby, nbx), dtype=torch.float32, device=dev)
+
+    def row_of(k):
+        return (rank + world * k) % cfg["nscan"]
+
+    def step(k):
+        r = row_of(k)
+        p = d_pos[r * npos_step:(r + 1) * npos_step]
+        o = d_int[r * npos_step:(r + 1) * npos_step]
+        e = J.L.JMS_ScanGPUDevice(npos_step, p.data_ptr(), 0.0, npass, None, o.data_ptr(), d_bin.data_ptr(), bin_)
+        if e != 0:
+            raise RuntimeError(f"JMS_ScanGPUDevice returned {e}")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            step(k)
+    torch.cuda.synchronize()
+    barrier()
+    l0 = J.L.JMS_KernelLaunches()
+    J.L.JMS_SetPassTiming(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for k in range(args.steps):
+                step(args.warmup + k)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = J.L.JMS_KernelLaunches() - l0
+    import ctypes as C
+    mc, mr = C.c_double(0), C.c_double(0)
+    nc, nr = C.c_longlong(0), C.c_longlong(0)
+    J.L.JMS_PassTiming(C.byref(mc), C.byref(nc), C.byref(mr), C.byref(nr))
+    J.L.JMS_SetPassTiming(0)
+    barrier()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps * steps_per_bench_step / (ms / 1e3)
+
+    # e2e through the host-buffer entry point (pinned host memory)
+    h_pos = torch.from_numpy(pos[:npos_step].copy()).pin_memory()
+    h_int = torch.zeros((npos_step, nd, ndet), dtype=torch.float32).pin_memory()
+    h_bin = torch.zeros((npos_step, nby, nbx), dtype=torch.float32).pin_memory()
+    fp = C.POINTER(C.c_float)
+
+    def e2e_step():
+        e = J.L.JMS_ScanGPU(npos_step, C.cast(h_pos.data_ptr(), fp), 0.0, npass, None,
+                            C.cast(h_int.data_ptr(), fp), C.cast(h_bin.data_ptr(), fp), bin_)
+        if e != 0:
+            raise RuntimeError(f"JMS_ScanGPU returned {e}")
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * e2e_steps * steps_per_bench_step / e2e_s
+
+    if rank == 0:
+        N = cfg["nx"] * cfg["ny"]
+        hbm, src = peaks()
+        # dominant pass: algorithmic bytes per launch = waves x 24 N (8N wave
+        # read + 8N wave write + 8N grating or propagator read)
+        waves = min(args.batch, npos_step)
+        kind, t_ms, n = ("row", mr.value, nr.value) if mr.value >= mc.value else ("column", mc.value, nc.value)
+        avg_s = (t_ms / max(n, 1)) / 1e3
+        algo = waves * 24 * N
+        achieved = algo / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": f"k_{kind}_pass<16,32> ({waves} waves)", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{src} hbm_gbs",
+                "traffic": traffic_from_profiles(kind), "bytes_per_launch": algo,
+                "avg_launch_us": avg_s * 1e6, "col_pass_us": 1e3 * mc.value / max(nc.value, 1),
+                "row_pass_us": 1e3 * mr.value / max(nr.value, 1)}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "STEM scan row: 64 probe positions x 16 frozen-phonon passes x 200 slices, "
+                                       "512x512 complex64, 3 annular detectors every 20 slices + 128x128 binned "
+                                       "exit diffraction",
+                           "grid": 512, "slices": cfg["nobj"], "positions_per_step": npos_step, "passes": npass,
+                           "batch_waves": args.batch, "parallelism": f"probe positions sharded over {world} GPU(s)",
+                           "l2": "inputs larger than L2 (128 MiB grating pool, 64 MiB of waves per batch)"},
+                "e2e": {"value": e2e_value, "unit": UNIT,
+                        "h2d_bytes_per_step": int(h_pos.numel() * 4),
+                        "d2h_bytes_per_step": int(h_int.numel() * 4 + h_bin.numel() * 4)},
+                "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
+        if world == 1 and not args.no_cpu:
+            try:
+                nt = host_threads()
+                sample = max(2 * nt, 8)
+                r, dt, _ = reference_cpu(cfg, sp, probe, pro, dets, pos, nt, sample)
+                line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nt, "kind": "reference",
+                                        "sample": f"{sample} probe positions x 1 phonon pass x 200 slices "
+                                                  f"({dt:.1f} s, CJMultiSlice::CPUMultislice on MKL, "
+                                                  "one thread per position)"}
+            except Exception as ex:
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                        "sample": f"not run: {ex}"}
+        if world == 1 and not args.no_err:
+            line["err_vs_fp64"] = error_vs_oracle(J, cfg, sp, probe, pro, dets, pos)
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def traffic_from_profiles(kind):
+    """DRAM bytes per launch of the pass, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"{kind}_pass_512.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch_scaled:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
+    """Relative error of the integrated detector signals of one probe position
+    (one phonon pass, 200 slices) against the FP64 oracle."""
+    try:
+        from oracle import oracle as OR
+    except Exception as ex:
+        return {"det_rel": None, "sample": f"oracle unavailable: {ex}"}
+    objslc = np.arange(cfg["nobj"]) % cfg["nslice_types"]
+    rng = OR.Rng(99)
+    var = rng.variant_sequence([cfg["nvar"]] * cfg["nslice_types"], objslc)
+    p = pos[len(pos) // 2:len(pos) // 2 + 1]
+    e, out, _ = J.scan(p, 1, varseq=var[None, :])
+    assert e == 0
+    n, hsh = OR.detection_planes(cfg["ndetper"], cfg["nobj"])
+    wl = J.L.GetWaveLength()
+    w0 = OR.offset(probe, sp.a, sp.b, wl, float(p[0, 0]), float(p[0, 1]))
+    res = OR.multislice(w0, np.concatenate(sp.gratings), objslc * cfg["nvar"] + var, pro[None],
+                        np.zeros(cfg["nobj"], np.int32), hsh, n, det=np.stack([d for d, _ in dets]),
+                        masks=[m for _, m in dets], imagedet=1)
+    ref = res["det_int"]
+    den = np.maximum(np.abs(ref).max(axis=0), 1e-30)
+    rel = float((np.abs(out[0] - ref).max(axis=0) / den).max())
+    return {"det_rel": rel, "sample": "1 position x 1 phonon pass x 200 slices, 11 planes x 3 detectors"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-err", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

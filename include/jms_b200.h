@@ -1,0 +1,168 @@
+/*
+ * jms_b200.h -- C ABI of the B200 multislice library (libjms_b200.so).
+ *
+ * Drop-in for the GPU multislice path of JMultiSliceLib's flat interface
+ * (src/JMultiSliceLib.h:108-380): the same symbol names, argument meanings,
+ * flag values, result layouts and integer error codes (0 = success), exported
+ * as plain extern "C" without __stdcall/__declspec.  Each declaration names
+ * the reference entry point it replaces (src/JMultiSliceLib.h:<line>).
+ *
+ * Conventions
+ *   - complex arrays are interleaved float pairs (re, im), row-major [ny][nx]
+ *     with x fastest, Fourier space in scrambled (FFT) order, as fcmplx in the
+ *     reference;
+ *   - C++ references of the reference interface become pointers here
+ *     (GetGridSize, GetGPUStats, CalculateRingDetector's msklen), the
+ *     std::string profile name becomes const char*, and CJProbeParams*
+ *     becomes JMSProbeParams* (its public data members, same order);
+ *   - whichcode: 1 = CPU, 2 = GPU.  This library has no CPU code path: any call
+ *     with the CPU bit set returns 1 and does nothing (CPUMultislice,
+ *     SetIncomingWaveCPU and ClearDetMem_h always return 1);
+ *   - all device memory is owned by the library; inputs are copied at Set*,
+ *     results are copied out by GetResult / GetAvgResult;
+ *   - one library instance (like the reference's static CJMultiSlice) serves
+ *     the flat calls; calls are not re-entrant.
+ */
+#ifndef JMS_B200_H
+#define JMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* flag values (src/JMultiSlice.h:126-149) */
+#define JMS_CODE_CPU            1
+#define JMS_CODE_GPU            2
+#define JMS_DETECT_INTEGRATED   1
+#define JMS_DETECT_IMAGE        2
+#define JMS_DETECT_DIFFRACTION  4
+#define JMS_DETECT_WAVEREAL     8
+#define JMS_DETECT_WAVEFOURIER  16
+#define JMS_DETECT_IMAGE_AVG    32
+#define JMS_DETECT_DIFFR_AVG    64
+#define JMS_DETECT_WAVER_AVG    128
+#define JMS_DETECT_WAVEF_AVG    256
+#define JMS_ACCMODE_NONE        0
+#define JMS_ACCMODE_INTEGRATE   1
+
+/* public data of CJProbeParams (src/JProbeGen.h:60-94), same order */
+typedef struct JMSProbeParams {
+	float m_wl;                 /* wavelength [nm] (replaced by the library's) */
+	float m_alpha;              /* convergence semi-angle [mrad] */
+	float m_alpha_rs;           /* relative aperture edge smoothness */
+	float m_alpha_x0, m_alpha_y0; /* aperture centre [mrad] */
+	float m_alpha_asym;         /* relative aperture asymmetry */
+	float m_alpha_adir;         /* asymmetry direction [deg] */
+	float m_btx, m_bty;         /* beam tilt [mrad] */
+	float m_source_width;       /* unused by the wave calculation */
+	int m_source_shape;         /* unused by the wave calculation */
+	float m_fspread_width;      /* unused by the wave calculation */
+	float m_fspread_kernel_width; /* unused by the wave calculation */
+	int m_fspread_kernel_samples; /* unused by the wave calculation */
+	float* m_abrr_coeff;        /* 2 * 24 aberration coefficients (x, y) [nm] */
+} JMSProbeParams;
+
+/* ---- basic interface ---------------------------------------------------- */
+float GetJMSVersion(void);                       /* src/JMultiSliceLib.h:111 */
+int SetJMSDebugLevel(int debuglevel);            /* src/JMultiSliceLib.h:114 */
+void SeedRngEx(int rngseed);                     /* src/JMultiSliceLib.h:123 */
+
+/* ---- physics interface ---------------------------------------------------- */
+float SetHighTension(float ht);                  /* src/JMultiSliceLib.h:129 */
+float GetHighTension(void);                      /* src/JMultiSliceLib.h:132 */
+float GetWaveLength(void);                       /* src/JMultiSliceLib.h:135 */
+void SetSupercellSize(float* a0);                /* src/JMultiSliceLib.h:138 */
+void SetSupercellSizeABC(float a, float b, float c); /* src/JMultiSliceLib.h:141 */
+void SetSliceThickness(int islc, float fthickness);  /* src/JMultiSliceLib.h:146 */
+void DiffractionDescan(int bActivate);           /* src/JMultiSliceLib.h:149 (bool) */
+void SetPlasmonMC(int bActivate, float fq_e, float fq_c, float fmfp, unsigned int nexmax); /* :152; activating it makes GPUMultislice return 5 */
+void SetDiffractionDescanN(int whichcode, int ndescanx, int ndescany, int iThread);       /* :160 */
+void SetDiffractionDescan(int whichcode, float descanx, float descany, int iThread);     /* :168 */
+void SetDiffractionDescanMRad(int whichcode, float descanx, float descany, int iThread); /* :176 */
+
+/* ---- numerics interface --------------------------------------------------- */
+void SetGridSize(int nx, int ny);                /* src/JMultiSliceLib.h:183 */
+void GetGridSize(int* nx, int* ny);              /* src/JMultiSliceLib.h:186 (int& -> int*) */
+int GetDetetionSliceNum(void);                   /* src/JMultiSliceLib.h:189 */
+int GetDetNum(void);                             /* src/JMultiSliceLib.h:192 */
+int GetCPUNum(void);                             /* src/JMultiSliceLib.h:195 */
+int GetGPUNum(void);                             /* src/JMultiSliceLib.h:198 */
+int GetGPUName(int idev, char* name);            /* src/JMultiSliceLib.h:201 (name: 256 bytes) */
+int GetCurrentGPU(void);                         /* src/JMultiSliceLib.h:204 */
+int SetCurrentGPU(int idev);                     /* src/JMultiSliceLib.h:207 */
+int GetGPUStats(int idev, int* iCMajor, int* iCMinor, int* iMaxThread, int64_t* CUDAmemtotal,
+	int64_t* CUDAmemfree);                       /* src/JMultiSliceLib.h:210 (refs -> pointers) */
+int GetUnscrambleHash(unsigned int* phash);      /* src/JMultiSliceLib.h:220 */
+float GetImageAveragingWeight(int whichcode, int iThread); /* src/JMultiSliceLib.h:223 */
+float GetWaveAveragingWeight(int whichcode, int iThread);  /* src/JMultiSliceLib.h:226 */
+
+/* ---- setup interface ------------------------------------------------------ */
+int PhaseGratingSetup(int whichcode, int nx, int ny, int nslc, int nvarmax, int* nslcvar); /* :231 */
+int ObjectSliceSetup(int nobjslc, int* objslc);  /* src/JMultiSliceLib.h:234 */
+int PropagatorSetup(int whichcode, int npro, int* proidx); /* src/JMultiSliceLib.h:237 */
+int DetectorSetup(int whichcode, int ndetper, int ndetint, int imagedet, int nthreads_CPU); /* :240; ndetint <= 8 */
+int InitCore(int whichcode, int nCPUthreads);    /* src/JMultiSliceLib.h:243 */
+int SetIncidentWave(int whichcode, float* wav);  /* src/JMultiSliceLib.h:246 */
+int SetIncidentWavePhaseplate(int whichcode, float* ppl, int bTranspose); /* src/JMultiSliceLib.h:249 */
+int ZeroIncidentWavePhaseplate(int whichcode);   /* src/JMultiSliceLib.h:252 */
+int SetSlicePhaseGratings(int whichcode, int islc, int nvar, float* pgr); /* src/JMultiSliceLib.h:255 */
+int SetPropagatorData(int whichcode, int ipro, float* pro); /* src/JMultiSliceLib.h:258 */
+int SetDetectorData(int whichcode, int idet, float* det, int msklen, int* msk); /* src/JMultiSliceLib.h:261 */
+int SetGPUPgrLoading(int npgrload);              /* src/JMultiSliceLib.h:266 (accepted, gratings stay on the device) */
+int ResetImageAveraging(int whichcode, int iThread); /* src/JMultiSliceLib.h:269 */
+int ResetWaveAveraging(int whichcode, int iThread);  /* src/JMultiSliceLib.h:272 */
+
+/* ---- calculation interface ------------------------------------------------ */
+int CalculateProbeWaveFourier(JMSProbeParams* prm, float* wav); /* src/JMultiSliceLib.h:280 */
+int SetIncomingWaveGPU(float* wav, int bTranspose);   /* src/JMultiSliceLib.h:286 */
+int SetIncomingWaveCPU(float* wav, int bTranspose, int iThread); /* src/JMultiSliceLib.h:293; returns 1 */
+int CalculatePropagator(float fthick, float otx, float oty, float* pro, int ntype); /* src/JMultiSliceLib.h:303 */
+int CalculateRingDetector(float beta0, float beta1, float phi0, float phi1, float theta0x, float theta0y,
+	const char* sdsprofile, float* det, int* msklen, int* msk, int kmom1); /* src/JMultiSliceLib.h:318 */
+int OffsetIncomingWave(int whichcode, float dx, float dy, float dz, int iThread, int ibtx, int ibty); /* :326 */
+int CPUMultislice(int islc0, int accmode, float weight, int iThread); /* src/JMultiSliceLib.h:333; returns 1 */
+int GPUMultislice(int islc0, int accmode, float weight); /* src/JMultiSliceLib.h:339 */
+int GetResult(int whichcode, int whichresult, float* dst, int iThread); /* src/JMultiSliceLib.h:346 */
+int GetAvgResult(int whichcode, int whichresult, float* dst, float* wgt, int iThread); /* src/JMultiSliceLib.h:354 */
+int ClearDetMem_h(int iThread);                  /* src/JMultiSliceLib.h:357; returns 1 */
+int ClearDetMem_d(void);                         /* src/JMultiSliceLib.h:363 */
+
+/* ---- cleanup interface ---------------------------------------------------- */
+int Cleanup(void);                               /* src/JMultiSliceLib.h:375 */
+void FreeLibMem(void);                           /* src/JMultiSliceLib.h:380 */
+
+/* ---- additions (no counterpart in the reference interface) ---------------- */
+/* Runs the library's kernels on the given CUDA stream (cudaStream_t passed as
+ * void*; NULL selects the library's own stream). */
+int JMS_SetStream(void* stream);
+/* Batched STEM scan on the current setup: npos probe positions pos[2*i] = dx,
+ * pos[2*i+1] = dy [nm] (defocus dz [nm] for all), each averaged over npass
+ * frozen-phonon passes (weight 1/npass).  varseq: npass x nobjslc variant
+ * indices, or NULL to draw them like GPUMultislice.  Host buffers:
+ * out_int [npos][ndetslc][ndet]; out_bin [npos][ny/bin][nx/bin] unscrambled
+ * exit-plane diffraction binned bin x bin (NULL to skip). */
+int JMS_ScanGPU(int npos, const float* pos, float dz, int npass, const int* varseq, float* out_int,
+	float* out_bin, int bin);
+/* The same with device buffers, asynchronous on the library stream;
+ * d_out_int is double [npos][ndetslc][ndet] and is accumulated into. */
+int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const int* varseq, double* d_out_int,
+	float* d_out_bin, int bin);
+/* Probe positions processed together in one pass sequence (default 32). */
+int JMS_SetScanBatch(int nwave);
+/* Kernel launches issued by the library so far. */
+long long JMS_KernelLaunches(void);
+/* Per-pass device timing: while on, each column and row pass launch is
+ * bracketed by CUDA events on the library stream; JMS_PassTiming returns the
+ * summed milliseconds and launch counts since the last JMS_SetPassTiming. */
+void JMS_SetPassTiming(int on);
+int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row);
+/* 1 if both grid lengths are supported by the fused passes. */
+int JMS_GridSupported(int nx, int ny);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JMS_B200_H */

@@ -1,0 +1,67 @@
+"""Build recipe of libjms_b200.so (sm_100a) -- run ``python -m jmultislicelib_b200.build``.
+
+Compiles the CUDA passes and the C++ host library in csrc/ with nvcc for
+sm_100a only and links them into jmultislicelib_b200/libjms_b200.so (in tree,
+next to this file), exporting the C ABI of include/jms_b200.h.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libjms_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT}/include"]
+SOURCES = ["jms_kernels.cu", "jms_host.cpp", "jms_generators.cpp", "jms_capi.cpp"] + [
+    f"jms_inst_{k}.cu" for k in range(7)]
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _headers() -> list[str]:
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    return hs + [os.path.join(ROOT, "include", "jms_b200.h")]
+
+
+def _compile(src: str, verbose: bool) -> str:
+    s = os.path.join(CSRC, src)
+    o = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
+    if _newer(o, [s] + _headers()):
+        cmd = [NVCC, *ARCH, *COMMON, "-c", s, "-o", o]
+        if verbose and src.endswith(".cu"):
+            cmd.insert(1, "-Xptxas=-v")
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr[-4000:]}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    return o
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    with cf.ThreadPoolExecutor(min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
+    if _newer(LIB, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

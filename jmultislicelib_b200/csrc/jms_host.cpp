@@ -1,0 +1,854 @@
+// jms_host.cpp -- setup chain, run loop and results of the B200 library.
+//
+// Follows the GPU branch of the reference class (src/JMultiSlice.cpp) for
+// status bits, error codes, buffer layouts and accumulation rules; the device
+// work is the fused pass sequence of jms_kernels.cu.  Deliberate differences
+// from the reference GPU branch (each covered by a test):
+//   - an integrating detector given without a mask is summed over the whole
+//     grid, as the reference CPU branch does (src/JMultiSlice.cpp:3411-3418);
+//     the reference GPU branch returns 0 for it because it always takes the
+//     masked sum with a zero-length mask (src/JMultiSlice.cpp:4288-4306);
+//   - integrated detector sums accumulate in FP64 on the device (the reference
+//     accumulates FP32 partial sums on the host, src/cu/reduction.cuh:113-126);
+//   - the probe-offset phase is reduced modulo 2 pi in FP64 before the FP32
+//     sincos (src/cu/ArrayOps.cu:410-421 forms it in FP32);
+//   - phase gratings always live in device memory; SetGPUPgrLoading(1) is
+//     accepted and changes nothing (180 GB of HBM hold any practical set).
+#include "jms_host.h"
+#include "jms_kernels.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+
+namespace jms {
+
+namespace {
+template <class T>
+void dfree(T*& p)
+{
+	if (p) cudaFree((void*)p);
+	p = nullptr;
+}
+} // namespace
+
+JmsB200::JmsB200()
+{
+	urng_.seed((unsigned)std::time(nullptr)); // CRng default: time-based seed
+	cudaGetDevice(&device_);
+}
+
+JmsB200::~JmsB200()
+{
+	SetPassTiming(0);
+	Cleanup();
+	dfree(d_twx_);
+	dfree(d_twy_);
+	dfree(d_work_);
+	dfree(d_partial_);
+	dfree(d_shift_);
+	if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+int JmsB200::post(cudaError_t e, const char* where)
+{
+	if (e != cudaSuccess) {
+		last_cuda_ = e;
+		std::fprintf(stderr, "Error: (%s): %s\n", where, cudaGetErrorString(e));
+	}
+	return e == cudaSuccess ? 0 : 1;
+}
+
+int JmsB200::SetStream(cudaStream_t s)
+{
+	if (own_stream_ && stream_) {
+		cudaStreamSynchronize(stream_);
+		cudaStreamDestroy(stream_);
+	}
+	stream_ = s;
+	own_stream_ = false;
+	return 0;
+}
+
+int JmsB200::SetCurrentGPU(int idev)
+{
+	int n = 0;
+	if (cudaGetDeviceCount(&n) != cudaSuccess || idev < 0 || idev >= n) return 1;
+	if (cudaSetDevice(idev) != cudaSuccess) return 2;
+	device_ = idev;
+	return 0;
+}
+
+int JmsB200::GetCurrentGPU() const
+{
+	int d = -1;
+	cudaGetDevice(&d);
+	return d;
+}
+
+void JmsB200::SetSliceThickness(int islc, float t)
+{
+	if (islc >= 0 && islc < nscslc_ && islc < (int)slcthick_.size()) slcthick_[islc] = t;
+}
+
+float JmsB200::GetSliceThickness(int islc) const
+{
+	if (islc >= 0 && islc < (int)slcthick_.size()) return slcthick_[islc];
+	return 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// random variants (src/JMultiSlice.cpp:1571-1676, src/rng.cpp:30-74)
+// ---------------------------------------------------------------------------
+void JmsB200::SeedRngEx(int nseed)
+{
+	urng_.seed(nseed == 0 ? (unsigned)std::time(nullptr) : (unsigned)nseed);
+}
+
+double JmsB200::unirand(double a, double b)
+{
+	return a + ((double)uni_(urng_) / (double)((unsigned long)0x7FFFFFFF)) * (b - a);
+}
+
+int JmsB200::GetRandomVariantSequence(int* out)
+{
+	if (!out) return 1;
+	if (nvarslc_.empty() || objslc_.empty() || nscslc_ < 1 || nobjslc_ < 1) return 2;
+	// per structure slice: a queue of unused variants; draw without
+	// replacement, and never start a refilled queue with the previous draw
+	int qmax = 1;
+	for (int v : nvarslc_) qmax = std::max(qmax, v);
+	std::vector<int> queue((size_t)nscslc_ * qmax, 0), left(nscslc_, 0), last(nscslc_, -1);
+	for (int i = 0; i < nobjslc_; i++) {
+		const int s = objslc_[i];
+		const int nv = nvarslc_[s];
+		if (nv < 2) { out[i] = 0; continue; }
+		int* q = &queue[(size_t)s * qmax];
+		if (left[s] <= 0) {
+			for (int j = 0; j < nv; j++) q[j] = j;
+			left[s] = nv;
+		}
+		int k = (int)unirand(0., (double)nv) % nv;
+		const int k0 = k;
+		while (q[k] < 0 || q[k] == last[s]) {
+			k = (k + 1) % nv;
+			if (k == k0) break;
+		}
+		int v = q[k];
+		if (v < 0) { // queue exhausted by the no-repeat rule: draw with replacement
+			v = (int)unirand(0.0, (double)nv);
+			left[s] = 0;
+		}
+		else {
+			q[k] = -1;
+			left[s]--;
+		}
+		last[s] = v;
+		out[i] = v;
+	}
+	return 0;
+}
+
+// ---------------------------------------------------------------------------
+// setup chain
+// ---------------------------------------------------------------------------
+int JmsB200::PhaseGratingSetup(int whichcode, int nx, int ny, int nslc, int nvarmax, const int* nslcvar)
+{
+	if (whichcode & CODE_CPU) return 1; // no CPU code path in this library
+	npgx_ = npgy_ = 0;
+	nscslc_ = 0;
+	nslcvar_ = 1;
+	nvarslc_.clear();
+	slcthick_.clear();
+	slcoffset_.clear();
+	dfree(d_pgr_);
+	status_gpu_ &= ~STATUS_PGR;
+	if (nslc >= 1 && nslcvar != nullptr) {
+		npgx_ = nx;
+		npgy_ = ny;
+		nscslc_ = nslc;
+		nslcvar_ = nvarmax;
+		nvarslc_.assign(nslcvar, nslcvar + nslc);
+		slcthick_.assign(nslc, 0.f);
+		slcoffset_.assign(nslc, 0);
+		long long off = 0;
+		for (int i = 0; i < nslc; i++) {
+			nvarslc_[i] = std::min(nvarslc_[i], nslcvar_);
+			slcoffset_[i] = off;
+			off += (long long)nvarslc_[i] * nx * ny;
+		}
+		if ((whichcode & CODE_GPU) && off > 0) {
+			if (post(cudaMalloc(&d_pgr_, sizeof(float2) * off), "PhaseGratingSetup")) return 104;
+			if (post(cudaMemset(d_pgr_, 0, sizeof(float2) * off), "PhaseGratingSetup")) return 104;
+		}
+	}
+	if (whichcode & CODE_GPU) status_gpu_ |= STATUS_PGR;
+	return 0;
+}
+
+int JmsB200::ObjectSliceSetup(int nobjslc, const int* objslc)
+{
+	nobjslc_ = 0;
+	objslc_.clear();
+	if (nobjslc >= 1 && objslc != nullptr) {
+		nobjslc_ = nobjslc;
+		objslc_.assign(objslc, objslc + nobjslc);
+	}
+	status_gpu_ |= STATUS_OBJ;
+	return 0;
+}
+
+int JmsB200::PropagatorSetup(int whichcode, int npro, const int* proidx)
+{
+	if (whichcode & CODE_CPU) return 1;
+	npro_ = 0;
+	if (npro >= 1 && proidx != nullptr) {
+		npro_ = npro;
+		proidx_.assign(proidx, proidx + nscslc_);
+		dfree(d_pro_);
+		const size_t n = (size_t)npro * nx_ * ny_;
+		if ((whichcode & CODE_GPU) && n > 0) {
+			if (post(cudaMalloc(&d_pro_, sizeof(float2) * n), "PropagatorSetup")) return 102;
+			if (post(cudaMemset(d_pro_, 0, sizeof(float2) * n), "PropagatorSetup")) return 102;
+		}
+	}
+	if (whichcode & CODE_GPU) status_gpu_ |= STATUS_PRO;
+	return 0;
+}
+
+int JmsB200::DetectorSetup(int whichcode, int ndetper, int ndetint, int imagedet, int nthreads_CPU)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if ((whichcode & CODE_GPU) && !(status_gpu_ & STATUS_OBJ)) {
+		std::fprintf(stderr, "Error: (DetectorSetup): no previous object slice setup for GPU code.\n");
+		return 101;
+	}
+	ndetper_ = std::max(0, ndetper);
+	det_objslc_.assign((size_t)nobjslc_ + 1, -1);
+	const int nd = SetDetectionPlanes(ndetper_, nobjslc_, det_objslc_.data());
+	return DetectorSetupList(whichcode, nullptr, -nd, ndetint, imagedet, nthreads_CPU);
+}
+
+int JmsB200::DetectorSetupList(int whichcode, const int* slc_det, int nlist, int ndetint, int imagedet, int)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if ((whichcode & CODE_GPU) && !(status_gpu_ & STATUS_OBJ)) return 101;
+	if (nlist >= 0) { // list overload (src/JMultiSlice.cpp:629-665)
+		ndetper_ = 0;
+		det_objslc_.assign((size_t)nobjslc_ + 1, -1);
+		ndetslc_ = SetDetectionPlanesList(slc_det, nlist, nobjslc_, det_objslc_.data());
+	}
+	else {
+		ndetslc_ = -nlist; // planes already placed by DetectorSetup
+	}
+	imagedet_ = imagedet;
+	ndet_ = 0;
+	detmask_len_.clear();
+	if (ndetint > 0) {
+		if (ndetint > kMaxDet) {
+			std::fprintf(stderr, "Error: (DetectorSetup): at most %d integrating detectors are fused per pass.\n", kMaxDet);
+			return 119;
+		}
+		ndet_ = ndetint;
+		detmask_len_.assign(ndet_, 0);
+	}
+	dfree(d_det_); dfree(d_detint_);
+	dfree(d_dif_); dfree(d_img_); dfree(d_wff_); dfree(d_wfr_);
+	dfree(d_dif_avg_); dfree(d_img_avg_); dfree(d_wff_avg_); dfree(d_wfr_avg_);
+	weight_imgavg_ = weight_wavavg_ = 0.f;
+	if ((whichcode & CODE_GPU) && imagedet_ > 0) {
+		const size_t N = (size_t)nx_ * ny_, L = N * (size_t)ndetslc_;
+		auto alloc = [&](void** p, size_t bytes, int code) -> int {
+			if (post(cudaMalloc(p, bytes), "DetectorSetup")) return code;
+			if (post(cudaMemset(*p, 0, bytes), "DetectorSetup")) return code;
+			return 0;
+		};
+		int e = 0;
+		if (ndet_ > 0 && (imagedet_ & DET_INTEGRATED)) {
+			if ((e = alloc((void**)&d_det_, sizeof(float) * ndet_ * N, 103))) return e;
+			if ((e = alloc((void**)&d_detint_, sizeof(double) * ndet_ * ndetslc_, 104))) return e;
+		}
+		if ((imagedet_ & DET_IMAGE) && (e = alloc((void**)&d_img_, sizeof(float) * L, 105))) return e;
+		if ((imagedet_ & DET_DIFFRACTION) && (e = alloc((void**)&d_dif_, sizeof(float) * L, 106))) return e;
+		if ((imagedet_ & DET_WAVEREAL) && (e = alloc((void**)&d_wfr_, sizeof(float2) * L, 107))) return e;
+		if ((imagedet_ & DET_WAVEFOURIER) && (e = alloc((void**)&d_wff_, sizeof(float2) * L, 109))) return e;
+		if ((imagedet_ & DET_IMAGE_AVG) && (e = alloc((void**)&d_img_avg_, sizeof(float) * L, 111))) return e;
+		if ((imagedet_ & DET_DIFFR_AVG) && (e = alloc((void**)&d_dif_avg_, sizeof(float) * L, 112))) return e;
+		if ((imagedet_ & DET_WAVER_AVG) && (e = alloc((void**)&d_wfr_avg_, sizeof(float2) * L, 114))) return e;
+		if ((imagedet_ & DET_WAVEF_AVG) && (e = alloc((void**)&d_wff_avg_, sizeof(float2) * L, 115))) return e;
+	}
+	if (whichcode & CODE_GPU) status_gpu_ |= STATUS_DET;
+	return 0;
+}
+
+int JmsB200::SetPhaseGratingData(int whichcode, int islc, int nvar, const float* pgr)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if (islc < 0 || islc >= nscslc_ || pgr == nullptr || nvarslc_.empty()) return 0;
+	const int nl = std::min(nvarslc_[islc], nvar);
+	if (nl < nvarslc_[islc]) nvarslc_[islc] = nl;
+	const size_t bytes = sizeof(float2) * (size_t)nl * npgx_ * npgy_;
+	if (bytes == 0) return 1;
+	if (d_pgr_ == nullptr) return 101;
+	if (post(cudaMemcpy(d_pgr_ + slcoffset_[islc], pgr, bytes, cudaMemcpyHostToDevice), "SetPhaseGratingData"))
+		return 102;
+	return 0;
+}
+
+int JmsB200::SetPropagatorData(int whichcode, int ipro, const float* pro)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if (ipro < 0 || ipro >= npro_ || pro == nullptr) return 0;
+	const size_t n = (size_t)nx_ * ny_;
+	if (n == 0) return 1;
+	if (d_pro_ == nullptr) return 101;
+	if (post(cudaMemcpy(d_pro_ + (size_t)ipro * n, pro, sizeof(float2) * n, cudaMemcpyHostToDevice), "SetPropagatorData"))
+		return 102;
+	return 0;
+}
+
+int JmsB200::SetDetectorData(int whichcode, int idet, const float* det, int msklen, const int* msk)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if (idet < 0 || idet >= ndet_ || det == nullptr) return 0;
+	const long N = (long)nx_ * ny_;
+	if (N == 0) return 1;
+	detmask_len_[idet] = (msk != nullptr && msklen > 0) ? msklen : 0;
+	if (d_det_ == nullptr) return 101;
+	// A mask restricts the readout sum to its entries (MaskedDotProduct,
+	// src/JMultiSlice.cpp:3303-3330); folding it into the detector function
+	// (each listed pixel counted as often as it is listed) gives the same sum
+	// from a full-grid pass.
+	std::vector<float> eff;
+	const float* src = det;
+	if (detmask_len_[idet] > 0) {
+		eff.assign(N, 0.f);
+		for (int k = 0; k < msklen; k++) {
+			const int m = msk[k];
+			if (m >= 0 && m < N) eff[m] += det[m];
+		}
+		src = eff.data();
+	}
+	if (post(cudaMemcpy(d_det_ + (size_t)idet * N, src, sizeof(float) * N, cudaMemcpyHostToDevice), "SetDetectorData"))
+		return 102;
+	return 0;
+}
+
+static void make_twiddles(std::vector<float2>& tw, int n)
+{
+	tw.resize(n);
+	for (int k = 0; k < n; k++) {
+		// exp(-2 pi i k/n) with the angle reduced in integers before the FP64 sincos
+		const double a = 6.283185307179586476925286766559 * (double)k / (double)n;
+		tw[k] = make_float2((float)std::cos(a), (float)(-std::sin(a)));
+	}
+}
+
+int JmsB200::InitCore(int whichcode, int)
+{
+	if (whichcode & CODE_CPU) return 1;
+	const int n = nx_ * ny_;
+	if (n > 0) {
+		fnx_.resize(nx_);
+		fny_.resize(ny_);
+		const int nx2 = (nx_ - (nx_ % 2)) >> 1, ny2 = (ny_ - (ny_ % 2)) >> 1;
+		for (int i = 0; i < nx_; i++) fnx_[i] = ((i + nx2) % nx_) - nx2;
+		for (int j = 0; j < ny_; j++) fny_[j] = ((j + ny2) % ny_) - ny2;
+	}
+	if ((whichcode & CODE_GPU) && (status_gpu_ & THRESHOLD_CORE) > 0 && n > 0) {
+		if (!pass_supported(nx_) || !pass_supported(ny_)) {
+			std::fprintf(stderr, "Error: (InitCore): grid %d x %d not supported by the fused passes.\n", nx_, ny_);
+			return 103;
+		}
+		if (!stream_) {
+			if (post(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "InitCore")) return 103;
+			own_stream_ = true;
+		}
+		weight_imgavg_ = weight_wavavg_ = 0.f;
+		dfree(d_wav0_); dfree(d_wav_); dfree(d_cppl_); dfree(d_twx_); dfree(d_twy_);
+		if (post(cudaMalloc(&d_wav0_, sizeof(float2) * n), "InitCore")) return 104;
+		if (post(cudaMalloc(&d_wav_, sizeof(float2) * n), "InitCore")) return 106;
+		if (post(cudaMalloc(&d_cppl_, sizeof(float) * n), "InitCore")) return 105;
+		cudaMemset(d_wav0_, 0, sizeof(float2) * n);
+		cudaMemset(d_wav_, 0, sizeof(float2) * n);
+		cudaMemset(d_cppl_, 0, sizeof(float) * n);
+		std::vector<float2> tw;
+		make_twiddles(tw, nx_);
+		if (post(cudaMalloc(&d_twx_, sizeof(float2) * nx_), "InitCore")) return 113;
+		cudaMemcpy(d_twx_, tw.data(), sizeof(float2) * nx_, cudaMemcpyHostToDevice);
+		make_twiddles(tw, ny_);
+		if (post(cudaMalloc(&d_twy_, sizeof(float2) * ny_), "InitCore")) return 114;
+		if (post(cudaMemcpy(d_twy_, tw.data(), sizeof(float2) * ny_, cudaMemcpyHostToDevice), "InitCore")) return 120;
+		status_gpu_ |= STATUS_CORE;
+	}
+	return 0;
+}
+
+static void transpose_into(std::vector<float2>& dst, const float2* src, int nx, int ny)
+{
+	// src holds nx rows of length ny; dst gets ny rows of length nx
+	dst.resize((size_t)nx * ny);
+	for (int j = 0; j < nx; j++)
+		for (int i = 0; i < ny; i++) dst[(size_t)j + (size_t)i * nx] = src[(size_t)i + (size_t)j * ny];
+}
+
+int JmsB200::SetIncidentWave(int whichcode, const float* wav, bool bTranspose)
+{
+	if (whichcode & CODE_CPU) return 1;
+	const int n = nx_ * ny_;
+	if ((status_gpu_ & THRESHOLD_CALC) > 0 && n > 0 && d_wav0_ && wav) {
+		std::vector<float2> t;
+		const void* src = wav;
+		if (bTranspose) { transpose_into(t, (const float2*)wav, nx_, ny_); src = t.data(); }
+		if (post(cudaMemcpy(d_wav0_, src, sizeof(float2) * n, cudaMemcpyHostToDevice), "SetIncidentWave")) return 102;
+	}
+	return 0;
+}
+
+int JmsB200::SetIncidentWavePhaseplate(int whichcode, const float* ppl, bool bTranspose)
+{
+	if (whichcode & CODE_CPU) return 1;
+	const int n = nx_ * ny_;
+	if ((status_gpu_ & THRESHOLD_CALC) > 0 && n > 0 && d_cppl_ && ppl) {
+		std::vector<float> t;
+		const float* src = ppl;
+		if (bTranspose) {
+			t.resize(n);
+			for (int j = 0; j < nx_; j++)
+				for (int i = 0; i < ny_; i++) t[(size_t)j + (size_t)i * nx_] = ppl[(size_t)i + (size_t)j * ny_];
+			src = t.data();
+		}
+		if (post(cudaMemcpy(d_cppl_, src, sizeof(float) * n, cudaMemcpyHostToDevice), "SetIncidentWavePhaseplate"))
+			return 102;
+	}
+	return 0;
+}
+
+int JmsB200::ZeroIncidentWavePhaseplate(int whichcode)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if ((status_gpu_ & THRESHOLD_CALC) > 0 && d_cppl_) {
+		if (post(cudaMemset(d_cppl_, 0, sizeof(float) * nx_ * ny_), "ZeroIncidentWavePhaseplate")) return 101;
+	}
+	return 0;
+}
+
+int JmsB200::GetUnscrambleHash(unsigned int* phash) const
+{
+	if (!phash) return 1;
+	if ((status_gpu_ & THRESHOLD_CALC) > 0 && (int)fnx_.size() == nx_ && (int)fny_.size() == ny_) {
+		const int nx2 = (nx_ - (nx_ % 2)) >> 1, ny2 = (ny_ - (ny_ % 2)) >> 1;
+		for (int j = 0; j < ny_; j++) {
+			const int ju = (fny_[j] + ny2) % ny_;
+			for (int i = 0; i < nx_; i++) {
+				const int iu = (fnx_[i] + nx2) % nx_;
+				phash[(size_t)ju * nx_ + iu] = (unsigned)((size_t)j * nx_ + i);
+			}
+		}
+	}
+	return 0;
+}
+
+int JmsB200::SetGPUPgrLoading(int) { return 0; }
+
+void JmsB200::SetDiffractionDescanN(int whichcode, int ndx, int ndy)
+{
+	if ((whichcode & CODE_CPU) || !(whichcode & CODE_GPU)) return;
+	if ((status_gpu_ & THRESHOLD_CALC) > 0) { descan_x_ = ndx; descan_y_ = ndy; }
+}
+
+void JmsB200::SetDiffractionDescan(int whichcode, float dkx, float dky)
+{
+	SetDiffractionDescanN(whichcode, (int)std::round(dkx * a0_[0]), (int)std::round(dky * a0_[1]));
+}
+
+void JmsB200::SetDiffractionDescanMRad(int whichcode, float dmx, float dmy)
+{
+	SetDiffractionDescan(whichcode, dmx * 0.001f / wl_, dmy * 0.001f / wl_);
+}
+
+// ---------------------------------------------------------------------------
+// calculation
+// ---------------------------------------------------------------------------
+int JmsB200::OffsetIncomingWave(int whichcode, float dx, float dy, float dz, int, int ibtx, int ibty, bool bcppl)
+{
+	if (whichcode & CODE_CPU) return 1;
+	if (nx_ * ny_ <= 0) return 1;
+	if (!((status_gpu_ & THRESHOLD_CALC) > 0) || !d_wav0_) return 0;
+	const double fz = (double)dz * (double)wl_ * 0.5;
+	const double a = a0_[0], b = a0_[1];
+	const double sh[4] = {(double)dx / a, (double)dy / b, fz / (a * a), fz / (b * b)};
+	if (post(launch_offset(d_wav_, d_wav0_, nx_, ny_, sh, bcppl ? d_cppl_ : nullptr, ibtx, ibty, stream_),
+		"OffsetIncomingWave"))
+		return 106;
+	launches_++;
+	return 0;
+}
+
+int JmsB200::SetIncomingWaveGPU(const float* wav, bool bTranspose)
+{
+	const int n = nx_ * ny_;
+	if (!((status_gpu_ & THRESHOLD_CALC) > 0) || n <= 0 || d_wav_ == nullptr) return 101;
+	std::vector<float2> t;
+	const void* src = wav;
+	if (bTranspose) { transpose_into(t, (const float2*)wav, nx_, ny_); src = t.data(); }
+	if (post(cudaMemcpyAsync(d_wav_, src, sizeof(float2) * n, cudaMemcpyHostToDevice, stream_), "SetIncomingWaveGPU"))
+		return 102;
+	cudaStreamSynchronize(stream_);
+	return 0;
+}
+
+int JmsB200::ensure_work(int nwave)
+{
+	if (nwave <= work_cap_ && d_work_) return 0;
+	dfree(d_work_);
+	work_cap_ = 0;
+	if (post(cudaMalloc(&d_work_, sizeof(float2) * (size_t)nwave * nx_ * ny_), "work buffer")) return 1;
+	work_cap_ = nwave;
+	return 0;
+}
+
+int JmsB200::ensure_partial(int nwave)
+{
+	const int nblk = row_blocks_per_wave(nx_, ny_);
+	const size_t need = (size_t)std::max(1, nwave) * std::max(1, ndetslc_) * std::max(1, ndet_) * std::max(1, nblk);
+	if (need <= partial_cap_ && d_partial_) return 0;
+	dfree(d_partial_);
+	partial_cap_ = 0;
+	if (post(cudaMalloc(&d_partial_, sizeof(float) * need), "partial sums")) return 1;
+	partial_cap_ = need;
+	return 0;
+}
+
+// Runs slices [islc0, nobjslc) on nwave waves sharing the variant sequence var.
+// Returns 0 or a stage code (1xx readout/entry, 4xx column pass, 6xx row
+// pass, 7xx detector reduction, 9xx exit image), following the stage offsets
+// of GPUMultislice (src/JMultiSlice.cpp:4611-4666).
+int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src,
+	const double* d_shift, int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx,
+	int nby)
+{
+	if (ensure_work(nwave) || ensure_partial(nwave)) return 1;
+	const long long N = (long long)nx_ * ny_;
+	const bool b_dif = (imagedet_ & (DET_INTEGRATED | DET_DIFFRACTION | DET_WAVEFOURIER | DET_DIFFR_AVG | DET_WAVEF_AVG)) != 0;
+	const bool b_img = (imagedet_ & (DET_IMAGE | DET_WAVEREAL | DET_IMAGE_AVG | DET_WAVER_AVG)) != 0;
+	const bool single = (nwave == 1) && (d_bin == nullptr);
+	const int ndet = (imagedet_ & DET_INTEGRATED) ? ndet_ : 0;
+	PassArgs base;
+	base.work = d_work_;
+	base.wstride = N;
+	base.nx = nx_;
+	base.ny = ny_;
+	base.nwave = nwave;
+	base.twx = d_twx_;
+	base.twy = d_twy_;
+	base.ndetslc = ndetslc_;
+	base.weight = weight;
+	base.ndet = (ndet > 0 && d_detint) ? ndet : 0;
+	base.det = d_det_;
+	base.partial = d_partial_;
+	base.nblk = row_blocks_per_wave(nx_, ny_);
+	base.chan_wstride = 0;
+	base.bin_out = d_bin;
+	base.bin = bin > 0 ? bin : 1;
+	base.nbx = nbx;
+	base.nby = nby;
+	base.bin_plane = nobjslc_ >= 0 && !det_objslc_.empty() ? det_objslc_[nobjslc_] : -1;
+	if (descan_on_) { base.descan_x = descan_x_; base.descan_y = descan_y_; }
+	PassArgs four = base, real = base;
+	if (single) {
+		four.dif = d_dif_; four.dif_avg = d_dif_avg_; four.wff = d_wff_; four.wff_avg = d_wff_avg_;
+		real.img = d_img_; real.img_avg = d_img_avg_; real.wfr = d_wfr_; real.wfr_avg = d_wfr_avg_;
+	}
+	cudaStream_t s = stream_;
+	if (base.ndet > 0) {
+		if (post(cudaMemsetAsync(d_partial_, 0, sizeof(float) * (size_t)nwave * ndetslc_ * ndet_ * base.nblk, s), "partials"))
+			return 101;
+	}
+	auto plane_of = [&](int p) { return (p >= 0 && p <= nobjslc_) ? det_objslc_[p] : -1; };
+	const int islc = std::min(std::max(islc0, 0), nobjslc_);
+	{ // entry: [offset] -> readout at plane islc -> IFT_x
+		PassArgs p = four;
+		p.wav0 = entry_src;
+		p.shift = d_shift;
+		p.cppl = d_shift ? d_cppl : nullptr;
+		p.ibtx = ibtx;
+		p.ibty = ibty;
+		p.plane = b_dif ? plane_of(islc) : -1;
+		if (post(launch_entry_rows(p, s), "GPUMultislice entry")) return 101;
+		launches_++;
+	}
+	for (int j = islc; j < nobjslc_; j++) {
+		const int st = objslc_[j] % nscslc_;
+		PassArgs c = real;
+		c.mul = d_pgr_ + slcoffset_[st] + (long long)var[j] * npgx_ * npgy_;
+		c.npgx = npgx_;
+		c.npgy = npgy_;
+		c.plane = b_img ? plane_of(j) : -1;
+		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
+		if (post(launch_col_pass(c, s), "GPUMultislice column pass")) return 401;
+		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
+		PassArgs r = four;
+		r.mul = d_pro_ + (long long)proidx_[st] * N;
+		r.plane = b_dif ? plane_of(j + 1) : -1;
+		r.store = (j + 1 < nobjslc_ || b_img) ? 1 : 0;
+		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
+		if (post(launch_row_pass(r, s), "GPUMultislice row pass")) return 601;
+		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
+		launches_ += 2;
+	}
+	if (b_img) { // exit plane image readout
+		PassArgs c = real;
+		c.plane = plane_of(nobjslc_);
+		if (post(launch_exit_cols(c, s), "GPUMultislice exit image")) return 901;
+		launches_++;
+	}
+	if (base.ndet > 0) {
+		if (post(launch_finalize(d_partial_, nwave, ndetslc_, ndet_, base.nblk, weight, d_detint, s), "detector sums"))
+			return 701;
+		launches_++;
+	}
+	return 0;
+}
+
+int JmsB200::GPUMultislice(int islc0, int accmode, float weight)
+{
+	if (d_wav_ == nullptr || nx_ * ny_ <= 0) return 1;
+	if (!(status_gpu_ & STATUS_CORE)) return 2;
+	if (plasmon_on_) {
+		std::fprintf(stderr, "Error: (GPUMultislice): plasmon Monte-Carlo shifts are not available in this library.\n");
+		return 5;
+	}
+	if (accmode == 0 && ClearDetMem_d() != 0) return 3;
+	const int islc = std::min(std::max(islc0, 0), nobjslc_);
+	std::vector<int> var((size_t)std::max(nobjslc_, 1), 0);
+	if (islc < nobjslc_) GetRandomVariantSequence(var.data()); // a new draw per run
+	int e = run_slices(1, islc, var.data(), weight, d_wav_, nullptr, 0, 0, nullptr, d_detint_, nullptr, 1, 0, 0);
+	if (e) return e;
+	if (imagedet_ & (DET_DIFFR_AVG | DET_IMAGE_AVG)) weight_imgavg_ += weight;
+	if (imagedet_ & (DET_WAVEF_AVG | DET_WAVER_AVG)) weight_wavavg_ += weight;
+	// the reference returns after the device work is done; execution errors are
+	// reported from here as well
+	if (post(cudaStreamSynchronize(stream_), "GPUMultislice")) return 201;
+	return 0;
+}
+
+int JmsB200::ClearDetMem_d()
+{
+	const size_t L = (size_t)nx_ * ny_ * ndetslc_;
+	cudaStream_t s = stream_;
+	if (d_detint_ && post(cudaMemsetAsync(d_detint_, 0, sizeof(double) * ndet_ * ndetslc_, s), "ClearDetMem_d")) return 3;
+	if (d_img_ && post(cudaMemsetAsync(d_img_, 0, sizeof(float) * L, s), "ClearDetMem_d")) return 3;
+	if (d_dif_ && post(cudaMemsetAsync(d_dif_, 0, sizeof(float) * L, s), "ClearDetMem_d")) return 3;
+	if (d_wfr_ && post(cudaMemsetAsync(d_wfr_, 0, sizeof(float2) * L, s), "ClearDetMem_d")) return 3;
+	if (d_wff_ && post(cudaMemsetAsync(d_wff_, 0, sizeof(float2) * L, s), "ClearDetMem_d")) return 3;
+	return 0;
+}
+
+int JmsB200::GetResult(int whichcode, int whichresult, float* dst, int)
+{
+	if (dst == nullptr) return 0;
+	if (whichcode & CODE_CPU) return 1;
+	if (!(whichcode & CODE_GPU) || ndetslc_ <= 0) return 0;
+	const size_t L = (size_t)nx_ * ny_ * ndetslc_;
+	cudaStreamSynchronize(stream_);
+	switch (whichresult) {
+	case DET_INTEGRATED: {
+		if (!d_detint_) return 0;
+		std::vector<double> h((size_t)ndet_ * ndetslc_);
+		if (post(cudaMemcpy(h.data(), d_detint_, sizeof(double) * h.size(), cudaMemcpyDeviceToHost), "GetResult")) return 0;
+		for (size_t k = 0; k < h.size(); k++) dst[k] = (float)h[k];
+		break;
+	}
+	case DET_IMAGE: if (d_img_) post(cudaMemcpy(dst, d_img_, sizeof(float) * L, cudaMemcpyDeviceToHost), "GetResult"); break;
+	case DET_DIFFRACTION: if (d_dif_) post(cudaMemcpy(dst, d_dif_, sizeof(float) * L, cudaMemcpyDeviceToHost), "GetResult"); break;
+	case DET_WAVEREAL: if (d_wfr_) post(cudaMemcpy(dst, d_wfr_, sizeof(float2) * L, cudaMemcpyDeviceToHost), "GetResult"); break;
+	case DET_WAVEFOURIER: if (d_wff_) post(cudaMemcpy(dst, d_wff_, sizeof(float2) * L, cudaMemcpyDeviceToHost), "GetResult"); break;
+	default: break;
+	}
+	return 0;
+}
+
+int JmsB200::GetAvgResult(int whichcode, int whichresult, float* dst, float* weight, int)
+{
+	if (weight) *weight = 0.f;
+	if (dst == nullptr) return 0;
+	if (whichcode & CODE_CPU) return 1;
+	if (!(whichcode & CODE_GPU) || ndetslc_ <= 0) return 0;
+	const size_t L = (size_t)nx_ * ny_ * ndetslc_;
+	cudaStreamSynchronize(stream_);
+	const void* src = nullptr;
+	size_t bytes = 0;
+	float w = 0.f;
+	switch (whichresult) {
+	case DET_IMAGE_AVG: src = d_img_avg_; bytes = sizeof(float) * L; w = weight_imgavg_; break;
+	case DET_DIFFR_AVG: src = d_dif_avg_; bytes = sizeof(float) * L; w = weight_imgavg_; break;
+	case DET_WAVER_AVG: src = d_wfr_avg_; bytes = sizeof(float2) * L; w = weight_wavavg_; break;
+	case DET_WAVEF_AVG: src = d_wff_avg_; bytes = sizeof(float2) * L; w = weight_wavavg_; break;
+	default: return 0;
+	}
+	if (src) post(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "GetAvgResult");
+	if (weight) *weight = w;
+	return 0;
+}
+
+float JmsB200::GetImageAveragingWeight(int whichcode, int) const { return (whichcode & CODE_GPU) ? weight_imgavg_ : 0.f; }
+float JmsB200::GetWaveAveragingWeight(int whichcode, int) const { return (whichcode & CODE_GPU) ? weight_wavavg_ : 0.f; }
+
+int JmsB200::ResetImageAveraging(int whichcode, int)
+{
+	const size_t L = (size_t)nx_ * ny_ * ndetslc_;
+	if (L == 0) return 0;
+	if (whichcode & CODE_GPU) {
+		weight_imgavg_ = 0.f;
+		if (d_img_avg_ && post(cudaMemsetAsync(d_img_avg_, 0, sizeof(float) * L, stream_), "ResetImageAveraging")) return 101;
+		if (d_dif_avg_ && post(cudaMemsetAsync(d_dif_avg_, 0, sizeof(float) * L, stream_), "ResetImageAveraging")) return 102;
+	}
+	return 0;
+}
+
+int JmsB200::ResetWaveAveraging(int whichcode, int)
+{
+	const size_t L = (size_t)nx_ * ny_ * ndetslc_;
+	if (L == 0) return 0;
+	if (whichcode & CODE_GPU) {
+		weight_wavavg_ = 0.f;
+		if (d_wfr_avg_ && post(cudaMemsetAsync(d_wfr_avg_, 0, sizeof(float2) * L, stream_), "ResetWaveAveraging")) return 103;
+		if (d_wff_avg_ && post(cudaMemsetAsync(d_wff_avg_, 0, sizeof(float2) * L, stream_), "ResetWaveAveraging")) return 104;
+	}
+	return 0;
+}
+
+cudaEvent_t JmsB200::timed_event()
+{
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+
+void JmsB200::SetPassTiming(int on)
+{
+	timing_on_ = on ? 1 : 0;
+	for (auto e : ev_col_) cudaEventDestroy(e);
+	for (auto e : ev_row_) cudaEventDestroy(e);
+	ev_col_.clear();
+	ev_row_.clear();
+}
+
+int JmsB200::PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row)
+{
+	if (stream_) cudaStreamSynchronize(stream_);
+	auto sum = [](const std::vector<cudaEvent_t>& ev, double* ms, long long* n) {
+		double t = 0.0;
+		for (size_t k = 0; k + 1 < ev.size(); k += 2) {
+			float x = 0.f;
+			if (cudaEventElapsedTime(&x, ev[k], ev[k + 1]) == cudaSuccess) t += x;
+		}
+		if (ms) *ms = t;
+		if (n) *n = (long long)(ev.size() / 2);
+	};
+	sum(ev_col_, ms_col, n_col);
+	sum(ev_row_, ms_row, n_row);
+	return 0;
+}
+
+void JmsB200::free_all()
+{
+	if (stream_) cudaStreamSynchronize(stream_);
+	dfree(d_pgr_); dfree(d_pro_); dfree(d_det_); dfree(d_wav0_); dfree(d_wav_); dfree(d_cppl_);
+	dfree(d_detint_); dfree(d_dif_); dfree(d_img_); dfree(d_wff_); dfree(d_wfr_);
+	dfree(d_dif_avg_); dfree(d_img_avg_); dfree(d_wff_avg_); dfree(d_wfr_avg_);
+}
+
+int JmsB200::Cleanup()
+{
+	free_all();
+	weight_imgavg_ = weight_wavavg_ = 0.f;
+	ndet_ = ndetper_ = ndetslc_ = 0;
+	imagedet_ = 0;
+	npro_ = 0;
+	nobjslc_ = 0;
+	npgx_ = npgy_ = nscslc_ = nslcvar_ = 0;
+	nvarslc_.clear(); objslc_.clear(); det_objslc_.clear(); proidx_.clear(); detmask_len_.clear();
+	slcoffset_.clear(); slcthick_.clear(); fnx_.clear(); fny_.clear();
+	status_gpu_ = 0;
+	return 0;
+}
+
+// ---------------------------------------------------------------------------
+// batched scan
+// ---------------------------------------------------------------------------
+int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const int* varseq, double* d_out_int,
+	float* d_out_bin, int bin)
+{
+	if (!((status_gpu_ & THRESHOLD_CALC) == THRESHOLD_CALC)) return 2;
+	if (npos <= 0 || npass <= 0 || d_pos == nullptr || nobjslc_ < 1) return 1;
+	if (d_out_bin && (bin <= 0 || nx_ % bin || ny_ % bin)) return 1;
+	const int nbx = d_out_bin ? nx_ / bin : 0, nby = d_out_bin ? ny_ / bin : 0;
+	if ((size_t)npos * 4 > shift_cap_) {
+		dfree(d_shift_);
+		shift_cap_ = 0;
+		if (post(cudaMalloc(&d_shift_, sizeof(double) * 4 * (size_t)npos), "ScanGPU")) return 1;
+		shift_cap_ = (size_t)npos * 4;
+	}
+	const double fz = (double)dz * (double)wl_ * 0.5;
+	if (post(launch_make_shift(d_shift_, d_pos, npos, a0_[0], a0_[1], fz, stream_), "ScanGPU")) return 1;
+	launches_++;
+	const int B = std::max(1, scan_batch_);
+	std::vector<int> var((size_t)nobjslc_);
+	const float w = 1.f / (float)npass;
+	for (int p0 = 0; p0 < npos; p0 += B) {
+		const int nw = std::min(B, npos - p0);
+		for (int ip = 0; ip < npass; ip++) {
+			if (varseq) std::memcpy(var.data(), varseq + (size_t)ip * nobjslc_, sizeof(int) * nobjslc_);
+			else GetRandomVariantSequence(var.data());
+			int e = run_slices(nw, 0, var.data(), w, d_wav0_, d_shift_ + (size_t)p0 * 4, 0, 0, d_cppl_,
+				d_out_int ? d_out_int + (size_t)p0 * ndetslc_ * ndet_ : nullptr,
+				d_out_bin ? d_out_bin + (size_t)p0 * nbx * nby : nullptr, bin, nbx, nby);
+			if (e) return e;
+		}
+	}
+	return 0;
+}
+
+int JmsB200::ScanGPU(int npos, const float* pos, float dz, int npass, const int* varseq, float* out_int,
+	float* out_bin, int bin)
+{
+	if (npos <= 0 || pos == nullptr) return 1;
+	float* d_pos = nullptr;
+	double* d_int = nullptr;
+	float* d_bin = nullptr;
+	const size_t nint = (size_t)npos * ndetslc_ * ndet_;
+	const size_t nb = out_bin && bin > 0 ? (size_t)npos * (nx_ / bin) * (ny_ / bin) : 0;
+	int e = 0;
+	cudaStream_t s = stream_;
+	if (post(cudaMallocAsync(&d_pos, sizeof(float) * 2 * npos, s), "ScanGPU")) return 1;
+	if (nint && post(cudaMallocAsync(&d_int, sizeof(double) * nint, s), "ScanGPU")) e = 1;
+	if (!e && nb && post(cudaMallocAsync(&d_bin, sizeof(float) * nb, s), "ScanGPU")) e = 1;
+	if (!e) {
+		cudaMemcpyAsync(d_pos, pos, sizeof(float) * 2 * npos, cudaMemcpyHostToDevice, s);
+		if (d_int) cudaMemsetAsync(d_int, 0, sizeof(double) * nint, s);
+		if (d_bin) cudaMemsetAsync(d_bin, 0, sizeof(float) * nb, s);
+		e = ScanGPUDevice(npos, d_pos, dz, npass, varseq, d_int, d_bin, bin);
+	}
+	if (!e && d_int && out_int) {
+		std::vector<double> h(nint);
+		cudaMemcpyAsync(h.data(), d_int, sizeof(double) * nint, cudaMemcpyDeviceToHost, s);
+		if (post(cudaStreamSynchronize(s), "ScanGPU")) e = 201;
+		for (size_t k = 0; k < nint; k++) out_int[k] = (float)h[k];
+	}
+	if (!e && d_bin && out_bin) {
+		cudaMemcpyAsync(out_bin, d_bin, sizeof(float) * nb, cudaMemcpyDeviceToHost, s);
+	}
+	if (post(cudaStreamSynchronize(s), "ScanGPU") && !e) e = 201;
+	cudaFreeAsync(d_pos, s);
+	if (d_int) cudaFreeAsync(d_int, s);
+	if (d_bin) cudaFreeAsync(d_bin, s);
+	cudaStreamSynchronize(s);
+	return e;
+}
+
+} // namespace jms

@@ -1,0 +1,190 @@
+// jms_host.h -- host side of the B200 multislice library.
+//
+// JmsB200 mirrors the GPU code path of the reference class CJMultiSlice
+// (src/JMultiSlice.h:185-738): the same setup chain and status bits, the same
+// generators, error codes and result layouts, with every computation on the
+// device done by the fused sm_100a passes of jms_kernels.cu.  The reference's
+// CPU code path (whichcode _JMS_CODE_CPU, CPUMultislice) is not part of this
+// library: calls that ask for it return error code 1.
+//
+// Beyond the reference interface it adds a batched scan entry point that runs
+// many probe positions and frozen-phonon passes through one stream.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace jms {
+
+// flags (numeric values of src/JMultiSlice.h:126-149)
+enum : int {
+	CODE_CPU = 1, CODE_GPU = 2,
+	STATUS_PGR = 1, STATUS_OBJ = 2, STATUS_PRO = 4, STATUS_DET = 8, STATUS_CORE = 16,
+	THRESHOLD_CORE = 15, THRESHOLD_CALC = 31,
+	DET_INTEGRATED = 1, DET_IMAGE = 2, DET_DIFFRACTION = 4, DET_WAVEREAL = 8, DET_WAVEFOURIER = 16,
+	DET_IMAGE_AVG = 32, DET_DIFFR_AVG = 64, DET_WAVER_AVG = 128, DET_WAVEF_AVG = 256,
+};
+
+// public probe parameters of CJProbeParams (src/JProbeGen.h:60-94)
+struct ProbeParams {
+	float wl = 0.001969f;       // wavelength [nm] (overwritten from the high tension)
+	float alpha = 0.025f;       // convergence semi-angle [mrad]
+	float alpha_rs = 0.03f;     // relative aperture edge smoothness
+	float alpha_x0 = 0.f, alpha_y0 = 0.f; // aperture centre [mrad]
+	float alpha_asym = 0.f;     // relative aperture asymmetry
+	float alpha_adir = 0.f;     // asymmetry direction [deg]
+	float btx = 0.f, bty = 0.f; // beam tilt [mrad]
+	float abrr[48] = {0};       // 24 aberrations (x, y) [nm], order of CJProbeGen's table
+};
+
+class JmsB200 {
+public:
+	JmsB200();
+	~JmsB200();
+	JmsB200(const JmsB200&) = delete;
+	JmsB200& operator=(const JmsB200&) = delete;
+
+	// ---- physics and grid (src/JMultiSlice.cpp:372-445)
+	float SetHighTension(float ht);
+	float GetHighTension() const { return ht_; }
+	float GetWaveLength() const { return wl_; }
+	void SetSupercellSize(float a, float b, float c) { a0_[0] = a; a0_[1] = b; a0_[2] = c; }
+	void GetSupercellSize(float* a0) const { a0[0] = a0_[0]; a0[1] = a0_[1]; a0[2] = a0_[2]; }
+	void SetGridSize(int nx, int ny) { nx_ = nx; ny_ = ny; }
+	void GetGridSize(int& nx, int& ny) const { nx = nx_; ny = ny_; }
+	void SetSliceThickness(int islc, float t);
+	float GetSliceThickness(int islc) const;
+	int GetDetetionSliceNum() const { return ndetslc_; }
+	int GetDetNum() const { return ndet_; }
+	int SetDetectionPlanes(int ndetper, int nobjslc, int* det_objslc) const;
+	int SetDetectionPlanesList(const int* slc_det, int nlist, int nobjslc, int* det_objslc) const;
+
+	// ---- diffraction descan (src/JMultiSlice.cpp:1108-1162) and plasmon switch
+	void DiffractionDescan(bool on) { descan_on_ = on ? 1 : 0; }
+	void SetDiffractionDescanN(int whichcode, int ndx, int ndy);
+	void SetDiffractionDescan(int whichcode, float dkx, float dky);
+	void SetDiffractionDescanMRad(int whichcode, float dmx, float dmy);
+	void SetPlasmonMC(bool use, unsigned int nexmax) { plasmon_on_ = (use && nexmax > 0) ? 1 : 0; }
+
+	// ---- generators (host, as in the reference)
+	int CalculateProbeWaveFourier(const ProbeParams& prm, float* wav) const;
+	int CalculatePropagator(float fthick, float otx, float oty, float* pro, int ntype);
+	int CalculateRingDetector(float beta0, float beta1, float phi0, float phi1, float theta0x, float theta0y,
+		const char* sdsprofile, float* det, int* msklen, int* msk, int kmom1) const;
+
+	// ---- setup chain (src/JMultiSlice.h:77-97)
+	int PhaseGratingSetup(int whichcode, int nx, int ny, int nslc, int nvarmax, const int* nslcvar);
+	int ObjectSliceSetup(int nobjslc, const int* objslc);
+	int PropagatorSetup(int whichcode, int npro, const int* proidx);
+	int DetectorSetup(int whichcode, int ndetper, int ndetint, int imagedet, int nthreads_CPU);
+	int DetectorSetupList(int whichcode, const int* slc_det, int nlist, int ndetint, int imagedet, int nthreads_CPU);
+	int SetPhaseGratingData(int whichcode, int islc, int nvar, const float* pgr);
+	int SetPropagatorData(int whichcode, int ipro, const float* pro);
+	int SetDetectorData(int whichcode, int idet, const float* det, int msklen, const int* msk);
+	int InitCore(int whichcode, int nCPUthreads);
+	int SetIncidentWave(int whichcode, const float* wav, bool bTranspose);
+	int SetIncidentWavePhaseplate(int whichcode, const float* ppl, bool bTranspose);
+	int ZeroIncidentWavePhaseplate(int whichcode);
+	int GetUnscrambleHash(unsigned int* phash) const;
+	int SetGPUPgrLoading(int npgrload);
+
+	// ---- RNG (src/rng.cpp:30-74 semantics)
+	void SeedRngEx(int nseed);
+	int GetRandomVariantSequence(int* out);
+
+	// ---- calculation
+	int OffsetIncomingWave(int whichcode, float dx, float dy, float dz, int iThread, int ibtx, int ibty, bool bcppl);
+	int SetIncomingWaveGPU(const float* wav, bool bTranspose);
+	int GPUMultislice(int islc0, int accmode, float weight);
+	int GetResult(int whichcode, int whichresult, float* dst, int iThread);
+	int GetAvgResult(int whichcode, int whichresult, float* dst, float* weight, int iThread);
+	float GetImageAveragingWeight(int whichcode, int iThread) const;
+	float GetWaveAveragingWeight(int whichcode, int iThread) const;
+	int ResetImageAveraging(int whichcode, int iThread);
+	int ResetWaveAveraging(int whichcode, int iThread);
+	int ClearDetMem_d();
+	int Cleanup();
+
+	// ---- device / stream
+	int SetStream(cudaStream_t s);
+	cudaStream_t Stream() const { return stream_; }
+	int SetCurrentGPU(int idev);
+	int GetCurrentGPU() const;
+
+	// ---- batched scan (addition): positions x frozen-phonon passes
+	// Host-buffer form: pos [npos][2] (dx, dy) nm; out_int [npos][ndetslc][ndet];
+	// out_bin [npos][ny/bin][nx/bin] (or null).  varseq [npass][nobjslc] or null
+	// (then one GetRandomVariantSequence draw per pass).  Each pass weighs 1/npass.
+	int ScanGPU(int npos, const float* pos, float dz, int npass, const int* varseq, float* out_int, float* out_bin,
+		int bin);
+	// Device-buffer form of the same (pointers on the device; asynchronous on
+	// the library stream).  out_int is double [npos][ndetslc][ndet].
+	int ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const int* varseq, double* d_out_int,
+		float* d_out_bin, int bin);
+	int SetScanBatch(int nwave) { scan_batch_ = nwave > 0 ? nwave : scan_batch_; return 0; }
+	int GetScanBatch() const { return scan_batch_; }
+	long long KernelLaunches() const { return launches_; }
+	// Per-pass device timing: with it on, every column / row pass launch is
+	// bracketed by CUDA events on the library stream; PassTiming sums them.
+	void SetPassTiming(int on);
+	int PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row);
+	int LastCudaError() const { return (int)last_cuda_; }
+
+private:
+	int gpu_ready(int need) const { return (status_gpu_ & need) == need; }
+	int post(cudaError_t e, const char* where);
+	int ensure_work(int nwave);
+	int ensure_partial(int nwave);
+	int run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src, const double* d_shift,
+		int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx, int nby);
+	void free_all();
+
+	// parameters
+	float ht_ = 0.f, wl_ = 0.f;
+	float a0_[3] = {0.f, 0.f, 0.f};
+	int nx_ = 0, ny_ = 0, npgx_ = 0, npgy_ = 0;
+	int nscslc_ = 0, nslcvar_ = 0, nobjslc_ = 0, npro_ = 0, nprotype_ = 0;
+	int ndet_ = 0, ndetper_ = 0, imagedet_ = 0, ndetslc_ = 0;
+	int status_gpu_ = 0;
+	std::vector<int> nvarslc_, objslc_, det_objslc_, proidx_, detmask_len_, fnx_, fny_;
+	std::vector<long long> slcoffset_;
+	std::vector<float> slcthick_;
+	// rng (CRng: std::mt19937, uniform ints 0..0x7FFFFFFF)
+	std::mt19937 urng_;
+	std::uniform_int_distribution<int> uni_{0, 0x7FFFFFFF};
+	double unirand(double a, double b);
+	// device
+	int device_ = 0;
+	cudaStream_t stream_ = nullptr;
+	bool own_stream_ = false;
+	float2* d_pgr_ = nullptr;      // phase gratings [sum nvar][npgy][npgx]
+	float2* d_pro_ = nullptr;      // propagators [npro][ny][nx]
+	float* d_det_ = nullptr;       // detector functions with masks folded in [ndet][ny][nx]
+	float2* d_wav0_ = nullptr;     // incident wave backup
+	float2* d_wav_ = nullptr;      // offset wave (input of GPUMultislice)
+	float* d_cppl_ = nullptr;      // constant phase plate
+	float2* d_twx_ = nullptr;      // twiddles exp(-2 pi i k/nx)
+	float2* d_twy_ = nullptr;
+	float2* d_work_ = nullptr;     // [work_cap_][ny][nx]
+	int work_cap_ = 0;
+	float* d_partial_ = nullptr;   // per-CTA detector partial sums
+	size_t partial_cap_ = 0;
+	double* d_detint_ = nullptr;   // single-run integrated detectors [ndetslc][ndet]
+	double* d_shift_ = nullptr;    // per-wave offsets (scan)
+	size_t shift_cap_ = 0;
+	float *d_dif_ = nullptr, *d_img_ = nullptr, *d_dif_avg_ = nullptr, *d_img_avg_ = nullptr;
+	float2 *d_wff_ = nullptr, *d_wfr_ = nullptr, *d_wff_avg_ = nullptr, *d_wfr_avg_ = nullptr;
+	float weight_imgavg_ = 0.f, weight_wavavg_ = 0.f;
+	int scan_batch_ = 32;
+	int descan_on_ = 0, descan_x_ = 0, descan_y_ = 0;
+	int timing_on_ = 0;
+	std::vector<cudaEvent_t> ev_col_, ev_row_;   // start/stop pairs
+	cudaEvent_t timed_event();
+	int plasmon_on_ = 0;
+	long long launches_ = 0;
+	cudaError_t last_cuda_ = cudaSuccess;
+};
+
+} // namespace jms

@@ -1,0 +1,119 @@
+// jms_kernels.cu -- size dispatch and the small kernels of the library
+// (per-run detector reduction, probe offset, scan offsets).
+#include "jms_fft.cuh"
+#include "jms_kernels.h"
+#include "jms_sizes.h"
+
+namespace jms {
+
+__device__ __forceinline__ float2 offset_factor_k(const double* sh, int i, int j, int nx, int ny, float cp)
+{
+	const int fi = (i + (nx >> 1)) % nx - (nx >> 1);
+	const int fj = (j + (ny >> 1)) % ny - (ny >> 1);
+	const double di = (double)fi, dj = (double)fj;
+	double t = di * sh[0] + dj * sh[1] + di * di * sh[2] + dj * dj * sh[3];
+	t -= floor(t);
+	float s, c;
+	if (cp != 0.f) sincosf(6.283185307179586f * (float)t + cp, &s, &c);
+	else sincospif(2.f * (float)t, &s, &c);
+	return make_float2(c, -s);
+}
+
+__global__ void k_make_shift(double* sh, const float* __restrict__ pos, int npos, double a, double b, double fz)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= npos) return;
+	sh[4 * i + 0] = (double)pos[2 * i] / a;
+	sh[4 * i + 1] = (double)pos[2 * i + 1] / b;
+	sh[4 * i + 2] = fz / (a * a);
+	sh[4 * i + 3] = fz / (b * b);
+}
+
+__global__ void k_finalize(const float* __restrict__ partial, int n, int nblk, float weight, double* det_int)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float* src = partial + (long long)i * nblk;
+	double s = 0.0;
+	for (int k = 0; k < nblk; k++) s += (double)src[k];
+	det_int[i] += (double)weight * s;
+}
+
+__global__ void k_offset(float2* out, const float2* __restrict__ wav0, int nx, int ny, double s0, double s1,
+	double s2, double s3, const float* __restrict__ cppl, int ibtx, int ibty)
+{
+	const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= (long long)nx * ny) return;
+	const int i = (int)(idx % nx), j = (int)(idx / nx);
+	const double sh[4] = {s0, s1, s2, s3};
+	int sx = (i - ibtx) % nx; if (sx < 0) sx += nx;
+	int sy = (j - ibty) % ny; if (sy < 0) sy += ny;
+	const float cp = cppl ? cppl[idx] : 0.f;
+	out[idx] = cmul(wav0[(long long)sy * nx + sx], offset_factor_k(sh, i, j, nx, ny, cp));
+}
+
+
+// ---------------------------------------------------------------------------
+// dispatch over supported line lengths
+// ---------------------------------------------------------------------------
+bool pass_supported(int n)
+{
+	switch (n) {
+#define X(n_, a_, b_) case n_: return true;
+		JMS_SIZES(X)
+#undef X
+	default: return false;
+	}
+}
+
+int row_blocks_per_wave(int nx, int ny)
+{
+	switch (nx) {
+#define X(n_, a_, b_) case n_: return row_blocks_t<a_, b_>(ny);
+		JMS_SIZES(X)
+#undef X
+	default: return 0;
+	}
+}
+
+#define JMS_DISPATCH(fn, len) \
+	switch (len) { \
+	JMS_SIZES(JMS_CASE_##fn) \
+	default: return cudaErrorInvalidValue; \
+	}
+#define JMS_CASE_entry(n_, a_, b_) case n_: return launch_entry_t<a_, b_>(p, s);
+#define JMS_CASE_row(n_, a_, b_) case n_: return launch_row_t<a_, b_>(p, s);
+#define JMS_CASE_col(n_, a_, b_) case n_: return launch_col_t<a_, b_>(p, s);
+#define JMS_CASE_exit(n_, a_, b_) case n_: return launch_exit_t<a_, b_>(p, s);
+
+cudaError_t launch_entry_rows(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(entry, p.nx) }
+cudaError_t launch_row_pass(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(row, p.nx) }
+cudaError_t launch_col_pass(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(col, p.ny) }
+cudaError_t launch_exit_cols(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(exit, p.ny) }
+
+cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
+	double* det_int, cudaStream_t s)
+{
+	const int n = nwave * ndetslc * ndet;
+	if (n <= 0) return cudaSuccess;
+	k_finalize<<<(n + 255) / 256, 256, 0, s>>>(partial, n, nblk, weight, det_int);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_make_shift(double* d_shift, const float* d_pos, int npos, double a, double b, double fz,
+	cudaStream_t s)
+{
+	k_make_shift<<<(npos + 127) / 128, 128, 0, s>>>(d_shift, d_pos, npos, a, b, fz);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_offset(float2* out, const float2* wav0, int nx, int ny, const double* sh, const float* cppl,
+	int ibtx, int ibty, cudaStream_t s)
+{
+	const long long n = (long long)nx * ny;
+	k_offset<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, wav0, nx, ny, sh[0], sh[1], sh[2], sh[3], cppl,
+		ibtx, ibty);
+	return cudaGetLastError();
+}
+
+} // namespace jms

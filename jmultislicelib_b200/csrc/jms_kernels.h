@@ -1,0 +1,86 @@
+// jms_kernels.h -- device-side entry points of the fused multislice passes.
+//
+// The multislice step of the reference (src/JMultiSlice.cpp:4590-4651:
+// [readout psi(k)] -> IFT -> [readout psi(r)] -> x t -> FT -> x P) is run as two
+// fused global passes over a batch of waves held [wave][ny][nx] (x fastest):
+//
+//   column pass  (one CTA = a tile of columns):  IFT_y -> [image readout]
+//                -> x t -> FT_y
+//   row pass     (one CTA = a tile of rows):     FT_x  -> x P (band limit is
+//                part of P) -> [Fourier readout] -> IFT_x
+//
+// Between the passes the wave is half transformed (x real / y Fourier after
+// the row pass, y Fourier / x real after the column pass), so each step reads
+// and writes the wave exactly twice.  An entry row pass applies the probe
+// offset and the entrance-plane readout, then IFT_x; an exit column pass
+// provides the exit-plane image readout.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace jms {
+
+constexpr int kMaxDet = 8;          // integrating detectors fused into one pass
+
+struct PassArgs {
+	float2* work = nullptr;         // [nwave][ny][nx] working waves
+	long long wstride = 0;          // elements between consecutive waves
+	int nx = 0, ny = 0, nwave = 0;
+	const float2* twx = nullptr;    // exp(-2 pi i k / nx), k < nx
+	const float2* twy = nullptr;    // exp(-2 pi i k / ny), k < ny
+	// multiplicative operand of this step
+	const float2* mul = nullptr;    // column pass: grating [npgy][npgx]; row pass: propagator [ny][nx]
+	int npgx = 0, npgy = 0;
+	// readout at this plane (-1 = none)
+	int plane = -1;
+	int ndetslc = 0;
+	float weight = 1.f;
+	int ndet = 0;                   // integrating detectors (0 = off)
+	const float* det = nullptr;     // [ndet][ny][nx], masks folded in
+	float* partial = nullptr;       // [nwave][ndetslc][ndet][nblk] per-CTA sums
+	int nblk = 0;                   // row-pass CTAs per wave
+	long long chan_wstride = 0;     // per-wave stride of full-size channels (0 = one shared channel)
+	float* dif = nullptr;           // Fourier channels [ndetslc][ny][nx]
+	float* dif_avg = nullptr;
+	float2* wff = nullptr;
+	float2* wff_avg = nullptr;
+	float* img = nullptr;           // real-space channels [ndetslc][ny][nx]
+	float* img_avg = nullptr;
+	float2* wfr = nullptr;
+	float2* wfr_avg = nullptr;
+	float* bin_out = nullptr;       // [nwave][nby][nbx] unscrambled, binned |psi(k)|^2
+	int bin = 1, nbx = 0, nby = 0;
+	int bin_plane = -1;             // plane at which the binned pattern is taken
+	int descan_x = 0, descan_y = 0; // integer-pixel diffraction descan of the Fourier readout
+	int store = 1;                  // row pass: 0 = stop after the readout (last slice)
+	// entry pass source: wav0 (nullptr = the work buffer); with shift set, wav0
+	// is the incident wave and each wave b gets its own probe offset
+	const float2* wav0 = nullptr;   // [ny][nx] Fourier space
+	const double* shift = nullptr;  // [nwave][4]: dx/a, dy/b, fz/a^2, fz/b^2 (phase in turns)
+	const float* cppl = nullptr;    // constant phase plate [ny][nx] or nullptr
+	int ibtx = 0, ibty = 0;         // beam tilt in Fourier pixels
+};
+
+// Supported line lengths: products of two factors <= 32 built from 2, 3, 5.
+bool pass_supported(int n);
+
+// launchers (return cudaSuccess or the launch error)
+cudaError_t launch_entry_rows(const PassArgs& p, cudaStream_t s);
+cudaError_t launch_row_pass(const PassArgs& p, cudaStream_t s);
+cudaError_t launch_col_pass(const PassArgs& p, cudaStream_t s);
+cudaError_t launch_exit_cols(const PassArgs& p, cudaStream_t s);
+int row_blocks_per_wave(int nx, int ny);
+
+// det_int[w][plane][d] += weight * sum_blk partial[w][plane][d][blk] (FP64)
+cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
+	double* det_int, cudaStream_t s);
+
+// shift[i] = (dx/a, dy/b, fz/a^2, fz/b^2) from pos[i] = (dx, dy) [nm]
+cudaError_t launch_make_shift(double* d_shift, const float* d_pos, int npos, double a, double b, double fz,
+	cudaStream_t s);
+
+// drop-in OffsetIncomingWave: out = wav0(k - tilt) * exp(-i(2 pi turns + cppl))
+cudaError_t launch_offset(float2* out, const float2* wav0, int nx, int ny, const double* shift_host4,
+	const float* cppl, int ibtx, int ibty, cudaStream_t s);
+
+} // namespace jms
