@@ -503,11 +503,12 @@ int JmsB200::SetIncomingWaveGPU(const float* wav, bool bTranspose)
 
 int JmsB200::ensure_work(int nwave)
 {
-	if (nwave <= work_cap_ && d_work_) return 0;
+	const size_t need = (size_t)nwave * nx_ * ny_; // elements; the grid may change between setups
+	if (need <= work_cap_ && d_work_) return 0;
 	dfree(d_work_);
 	work_cap_ = 0;
-	if (post(cudaMalloc(&d_work_, sizeof(float2) * (size_t)nwave * nx_ * ny_), "work buffer")) return 1;
-	work_cap_ = nwave;
+	if (post(cudaMalloc(&d_work_, sizeof(float2) * need), "work buffer")) return 1;
+	work_cap_ = need;
 	return 0;
 }
 

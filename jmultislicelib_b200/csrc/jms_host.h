@@ -167,8 +167,8 @@ private:
 	float* d_cppl_ = nullptr;      // constant phase plate
 	float2* d_twx_ = nullptr;      // twiddles exp(-2 pi i k/nx)
 	float2* d_twy_ = nullptr;
-	float2* d_work_ = nullptr;     // [work_cap_][ny][nx]
-	int work_cap_ = 0;
+	float2* d_work_ = nullptr;     // working waves [nwave][ny][nx]
+	size_t work_cap_ = 0;          // capacity in complex elements
 	float* d_partial_ = nullptr;   // per-CTA detector partial sums
 	size_t partial_cap_ = 0;
 	double* d_detint_ = nullptr;   // single-run integrated detectors [ndetslc][ndet]

@@ -248,9 +248,18 @@ class RefJMS:
 
 def cpu_scan(objs, npos_xy: np.ndarray, nrepeat: int, ndetout: int) -> tuple[np.ndarray, int]:
     """Run the reference multi-threaded CPU scan; one RefJMS per thread."""
+    import torch
+
     L = lib()
     arr = (C.c_void_p * len(objs))(*[o.h for o in objs])
     pos = np.ascontiguousarray(npos_xy, np.float32)
     out = np.zeros((pos.shape[0], ndetout), np.float32)
-    e = L.ref_cpu_scan(arr, len(objs), pos.shape[0], fptr(pos), nrepeat, ndetout, fptr(out))
+    # one MKL thread per transform (the reference links mkl_sequential); the
+    # parallelism is one worker thread per CJMultiSlice object
+    nt0 = torch.get_num_threads()
+    torch.set_num_threads(1)
+    try:
+        e = L.ref_cpu_scan(arr, len(objs), pos.shape[0], fptr(pos), nrepeat, ndetout, fptr(out))
+    finally:
+        torch.set_num_threads(nt0)
     return out, e

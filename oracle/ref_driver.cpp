@@ -120,7 +120,7 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	std::vector<std::thread> pool;
 	for (int t = 0; t < nthreads; t++) {
 		pool.emplace_back([&, t]() {
-			mkl_set_num_threads_local(1);
+			// MKL runs sequentially: the caller sets its global thread count to 1
 			RefJMS* jms = (RefJMS*)objs[t];
 			float w = 1.f / (float)nrepeat;
 			for (;;) {
