@@ -3,12 +3,24 @@
 // Included by the jms_inst_*.cu files, which instantiate the launchers for
 // their share of the supported line lengths; jms_kernels.cu dispatches on the
 // grid size.  See jms_kernels.h for the pass structure and jms_fft.cuh for the
-// line FFT.  Reference semantics followed here:
+// in-register DFTs.  Reference semantics followed here:
 //   slice loop order          src/JMultiSlice.cpp:4590-4651 (GPUMultislice)
 //   Fourier-space readout     src/JMultiSlice.cpp:4218-4367 (ReadoutDifDet_d)
 //   real-space readout        src/JMultiSlice.cpp:4369-4465 (ReadoutImgDet_d)
 //   grating multiply          src/cu/ArrayOps.cu:202-234 (MulKernel / sub-frame)
 //   probe offset              src/JMultiSlice.cpp:1961-2084, src/cu/ArrayOps.cu:340-421
+//
+// Line transforms.  A line of N = A*B points is held by B threads, thread j
+// owning x[j + B m] (m < A): loads and stores of that layout are coalesced.
+// A transform runs in two register stages around one shared-memory exchange
+// and leaves the line in a "middle" layout, where the pass applies its
+// elementwise work (x P and Fourier readout, or real-space readout and x t);
+// the opposite-direction transform then returns the line to the load layout.
+//   split 1 (A, B any):  the middle layout has A threads per line, thread k1
+//       holding X[k1 + A k2] (k2 < B); threads k1 >= A idle in the middle.
+//   split 2 (B = 2A):   the B-point stage is shared by a thread pair with a
+//       radix-2 step over warp shuffles, so every thread keeps A values in all
+//       stages: thread (k1, h) = 2 k1 + h holds X[k1 + A (k + A h)], k < A.
 #pragma once
 #include "jms_fft.cuh"
 #include "jms_kernels.h"
@@ -16,68 +28,208 @@
 namespace jms {
 
 // ---------------------------------------------------------------------------
-// line transforms with one shared-memory exchange (see jms_fft.cuh)
+// tiles: thread <-> (line, position) maps and exchange-buffer layouts
 // ---------------------------------------------------------------------------
-// Row tile: LINES rows, thread t -> (line = t / P, pos = t % P) for a role with
-// P threads per line; exchange buffer S(line, k1, j) padded to B+1.
+// Row tile: LINES rows per CTA; thread t -> (line t / P, position t % P).
 template <int LINES>
 struct RowTile {
+	static constexpr int kLines = LINES;
+	static constexpr int kPartner = 1;   // lane distance of positions 2k and 2k+1
 	template <int P>
 	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid / P; pos = tid % P; }
+	// split 1 exchange S(line, k1, j), k1 < A, j < B, rows padded to B+1
 	template <int A, int B>
-	__device__ __forceinline__ static int sidx(int line, int k1, int j) { return (line * A + k1) * (B + 1) + j; }
+	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return (line * A + k1) * (B + 1) + j; }
 	template <int A, int B>
-	static constexpr int sm_elems() { return LINES * A * (B + 1); }
+	static constexpr int sm_pad() { return LINES * A * (B + 1); }
+	// split 2 exchanges S(line, a, b), a < A, b < B, rows padded to B+2: the
+	// pair reads of a half warp (a = 0..7, b = 2i + h) land on 16 distinct
+	// bank pairs, and every per-thread loop has a constant address stride
+	//   forward: a = k1, b = j (written by j, read by the pair (k1, h) at j = 2i + h)
+	//   inverse: a = n1, b = q2 (written by the pair (n1, h) at q2 = 2m + h, read by q2)
+	template <int A, int B>
+	__device__ __forceinline__ static int s_fwd(int line, int a, int b) { return (line * A + a) * (B + 2) + b; }
+	template <int A, int B>
+	__device__ __forceinline__ static int s_inv(int line, int q2, int n1) { return (line * A + n1) * (B + 2) + q2; }
+	template <int A, int B>
+	static constexpr int sm_split() { return LINES * A * (B + 2); }
 };
 
-// Column tile: C columns, thread t -> (line = t % C, pos = t / C); exchange
-// buffer S(c, k1, j) with the column index fastest (padding keeps the k1
-// groups of a half warp on distinct banks when C < 16).
+// Column tile: C columns per CTA; thread t -> (column t % C, position t / C),
+// so a warp touches C consecutive complex values of a few rows.  Exchange
+// buffers keep the column index fastest; a pad of C complex per k1 block keeps
+// the k1 groups of a half warp on distinct banks when C < 16.
 template <int C>
 struct ColTile {
+	static constexpr int kLines = C;
+	static constexpr int kPartner = C;
 	static constexpr int PAD = (C < 16) ? C : 0;
 	template <int P>
 	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid % C; pos = tid / C; }
 	template <int A, int B>
-	__device__ __forceinline__ static int sidx(int line, int k1, int j) { return k1 * (B * C + PAD) + j * C + line; }
+	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return k1 * (B * C + PAD) + j * C + line; }
 	template <int A, int B>
-	static constexpr int sm_elems() { return A * (B * C + PAD); }
+	static constexpr int sm_pad() { return A * (B * C + PAD); }
+	template <int A, int B>
+	__device__ __forceinline__ static int s_fwd(int line, int k1, int j) { return k1 * (B * C + PAD) + j * C + line; }
+	template <int A, int B>
+	__device__ __forceinline__ static int s_inv(int line, int q2, int n1) { return n1 * (B * C + PAD) + q2 * C + line; }
+	template <int A, int B>
+	static constexpr int sm_split() { return A * (B * C + PAD); }
 };
 
-// One N = A*B point transform per line.  Input: role with B threads per
-// line, thread j holds v[m] = x[j + B m] (m < A).  Output: role with A threads
-// per line, thread k1 holds v[k2] = X[k1 + A k2] (k2 < B).  tw = exp(-2 pi i k/N).
-// act_in / act_out: this thread's line exists (all threads reach the barriers).
+// twiddle by table value w = exp(-2 pi i k / N) (conjugated for the inverse)
+template <bool INV>
+__device__ __forceinline__ float2 tw_mul(float2 v, float2 w) { return INV ? cmulc(v, w) : cmul(v, w); }
+
+// ---- split 1 -----------------------------------------------------------------
+// in: B threads/line, thread j holds x[j + B m] (m < A)
+// out: A threads/line, thread k1 holds X[k1 + A k2] (k2 < B)
 template <int A, int B, bool INV, class Tile, int RM>
-__device__ __forceinline__ void line_fft(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid,
-	int nlines_valid)
+__device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
 {
-	{
-		int line, j;
-		Tile::template role<B>(tid, line, j);
-		if (line < nlines_valid && j < B) {
-			dft_reg<A, 1, 0, INV>(v);
-			#pragma unroll
-			for (int k1 = 1; k1 < A; k1++) {
-				float2 w = __ldg(tw + j * k1); // j*k1 < N
-				v[k1] = INV ? cmulc(v[k1], w) : cmul(v[k1], w);
-			}
-			#pragma unroll
-			for (int k1 = 0; k1 < A; k1++) sm[Tile::template sidx<A, B>(line, k1, j)] = v[k1];
-		}
+	int line, j;
+	Tile::template role<B>(tid, line, j);
+	const bool in_role = line < Tile::kLines && j < B;
+	if (in_role) {
+		dft_reg<A, 1, 0, INV>(v);
+		#pragma unroll
+		for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + j * k1));
+		#pragma unroll
+		for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_pad<A, B>(line, k1, j)] = v[k1];
 	}
 	__syncthreads();
-	{
-		int line, k1;
-		Tile::template role<A>(tid, line, k1);
-		if (line < nlines_valid && k1 < A) {
-			#pragma unroll
-			for (int j = 0; j < B; j++) v[j] = sm[Tile::template sidx<A, B>(line, k1, j)];
-			dft_reg<B, 1, 0, INV>(v);
-		}
+	Tile::template role<A>(tid, line, j);
+	if (line < Tile::kLines && j < A) {
+		#pragma unroll
+		for (int jj = 0; jj < B; jj++) v[jj] = sm[Tile::template s_pad<A, B>(line, j, jj)];
+		dft_reg<B, 1, 0, INV>(v);
 	}
 	__syncthreads();
 }
+
+// in: A threads/line, thread k1 holds x[k1 + A k2] (k2 < B)
+// out: B threads/line, thread j holds y[j + B m] (m < A)
+template <int A, int B, bool INV, class Tile, int RM>
+__device__ __forceinline__ void fft_s1_inv(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+{
+	// the transpose of fft_s1_fwd: per-thread B-point DFT, exchange, A-point DFT
+	fft_s1_fwd<B, A, INV, Tile>(v, sm, tw, tid);
+}
+
+// ---- split 2 (B = 2A) ------------------------------------------------------------
+// in: B threads/line, thread j holds x[j + B m] (m < A)
+// out: B threads/line, thread (k1, h) = 2 k1 + h holds X[k1 + A (k + A h)] (k < A)
+template <int A, bool INV, class Tile, int RM>
+__device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+{
+	constexpr int B = 2 * A;
+	int line, j;
+	Tile::template role<B>(tid, line, j);
+	dft_reg<A, 1, 0, INV>(v);
+	#pragma unroll
+	for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + j * k1));
+	#pragma unroll
+	for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_fwd<A, B>(line, k1, j)] = v[k1];
+	__syncthreads();
+	const int k1 = j >> 1, h = j & 1;
+	#pragma unroll
+	for (int i = 0; i < A; i++) v[i] = sm[Tile::template s_fwd<A, B>(line, k1, 2 * i + h)];
+	dft_reg<A, 1, 0, INV>(v);
+	// radix-2 across the pair: Y[k] = E[k] + W_B^k O[k], Y[k + A] = E[k] - W_B^k O[k]
+	static_for<A>([&](auto K) {
+		constexpr int k = K.value;
+		float2 o;
+		o.x = __shfl_xor_sync(0xffffffffu, v[k].x, Tile::kPartner);
+		o.y = __shfl_xor_sync(0xffffffffu, v[k].y, Tile::kPartner);
+		const float2 e = h ? o : v[k];
+		const float2 t = twiddle_ct<k, B, INV>(h ? v[k] : o);
+		v[k] = h ? csub(e, t) : cadd(e, t);
+	});
+	__syncthreads();
+}
+
+// in: B threads/line, thread (n1, h) = 2 n1 + h holds x[n1 + A (k + A h)] (k < A)
+// out: B threads/line, thread j holds y[j + B m] (m < A)
+template <int A, bool INV, class Tile, int RM>
+__device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+{
+	constexpr int B = 2 * A;
+	int line, j;
+	Tile::template role<B>(tid, line, j);
+	const int n1 = j >> 1, h = j & 1;
+	// radix-2 decimation in frequency over n2 = k + A h across the pair
+	static_for<A>([&](auto K) {
+		constexpr int k = K.value;
+		float2 o;
+		o.x = __shfl_xor_sync(0xffffffffu, v[k].x, Tile::kPartner);
+		o.y = __shfl_xor_sync(0xffffffffu, v[k].y, Tile::kPartner);
+		v[k] = h ? twiddle_ct<k, B, INV>(csub(o, v[k])) : cadd(v[k], o);
+	});
+	dft_reg<A, 1, 0, INV>(v);   // output q2 = 2 m + h
+	#pragma unroll
+	for (int m = 0; m < A; m++) {
+		const int q2 = 2 * m + h;
+		if (n1 > 0) v[m] = tw_mul<INV>(v[m], __ldg(tw + n1 * q2));
+		sm[Tile::template s_inv<A, B>(line, q2, n1)] = v[m];
+	}
+	__syncthreads();
+	#pragma unroll
+	for (int i = 0; i < A; i++) v[i] = sm[Tile::template s_inv<A, B>(line, j, i)];
+	dft_reg<A, 1, 0, INV>(v);
+	__syncthreads();
+}
+
+// ---- plans -------------------------------------------------------------------------
+template <int A_, int B_>
+struct Plan {
+	static constexpr int A = A_, B = B_, N = A_ * B_;
+	static constexpr int S = (B_ == 2 * A_ && A_ >= 4) ? 2 : 1;
+	static constexpr int RM = (S == 2) ? A_ : (A_ > B_ ? A_ : B_);   // registers per thread (complex)
+	static constexpr int T = B_;                                       // threads per line (load layout)
+	static constexpr int TMID = (S == 2) ? B_ : A_;                    // threads per line (middle layout)
+	static constexpr int EMID = (S == 2) ? A_ : B_;                    // values per thread (middle layout)
+	static constexpr int TMAX = (T > TMID) ? T : TMID;
+	// line index of the e-th middle value of position pos
+	__device__ __forceinline__ static int mid(int pos, int e)
+	{
+		if constexpr (S == 2) return (pos >> 1) + A * (e + A * (pos & 1));
+		else return pos + A * e;
+	}
+	template <bool INV, class Tile>
+	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	{
+		if constexpr (S == 2) fft_s2_fwd<A, INV, Tile>(v, sm, tw, tid);
+		else fft_s1_fwd<A, B, INV, Tile>(v, sm, tw, tid);
+	}
+	template <bool INV, class Tile>
+	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	{
+		if constexpr (S == 2) fft_s2_inv<A, INV, Tile>(v, sm, tw, tid);
+		else fft_s1_inv<A, B, INV, Tile>(v, sm, tw, tid);
+	}
+	template <class Tile>
+	static constexpr int smem_elems()
+	{
+		if constexpr (S == 2) return Tile::template sm_split<A, B>();
+		else {
+			constexpr int a = Tile::template sm_pad<A, B>(), b = Tile::template sm_pad<B, A>();
+			return a > b ? a : b;
+		}
+	}
+};
+
+__host__ __device__ constexpr int gcd_ct(int a, int b) { return b == 0 ? a : gcd_ct(b, a % b); }
+// rows per row-pass CTA: about 256 threads, a whole number of warps
+template <class PL>
+__host__ __device__ constexpr int row_lines()
+{
+	constexpr int T = PL::TMAX;
+	constexpr int m = 32 / gcd_ct(T, 32);
+	constexpr int l = (256 / T) / m * m;
+	return l < m ? m : l;
+}
+constexpr int kColC = 16;
 
 // ---------------------------------------------------------------------------
 // readouts
@@ -176,230 +328,188 @@ __device__ __forceinline__ float2 offset_factor(const double* sh, int i, int j, 
 }
 
 // ---------------------------------------------------------------------------
-// pass kernels
+// pass kernels (template parameter: the line plan of the transformed axis)
 // ---------------------------------------------------------------------------
-template <int R1, int R2>
-struct Geo {
-	static constexpr int N = R1 * R2;
-	static constexpr int RM = R1 > R2 ? R1 : R2;
-};
-
-__host__ __device__ constexpr int gcd_ct(int a, int b) { return b == 0 ? a : gcd_ct(b, a % b); }
-// rows per row-pass CTA: about 256 threads, thread count a multiple of 32
-template <int R1, int R2>
-__host__ __device__ constexpr int row_lines()
-{
-	constexpr int RM = Geo<R1, R2>::RM;
-	constexpr int m = 32 / gcd_ct(RM, 32);
-	constexpr int l = (256 / RM) / m * m;
-	return l < m ? m : l;
-}
-constexpr int kColC = 16;
-
 // Entry row pass: [offset] -> Fourier readout (plane) -> IFT_x.
-template <int R1, int R2>
-__global__ void __launch_bounds__(row_lines<R1, R2>() * Geo<R1, R2>::RM)
+template <class PL>
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
 k_entry_rows(const PassArgs p)
 {
-	constexpr int N = R1 * R2, RM = Geo<R1, R2>::RM, L = row_lines<R1, R2>(), NT = L * RM;
+	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
 	using T = RowTile<L>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
 	float2* W = p.work + (long long)b * p.wstride;
-	float2 v[RM];
+	float2 v[PL::RM];
+	#pragma unroll
+	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
 	float acc[kMaxDet];
 	#pragma unroll
 	for (int d = 0; d < kMaxDet; d++) acc[d] = 0.f;
-	{
-		int line, j;
-		T::template role<R2>(tid, line, j);
-		if (line < nval) {
-			const int y = row0 + line;
-			#pragma unroll
-			for (int m = 0; m < R1; m++) {
-				const int kx = j + R2 * m;
-				float2 a;
-				if (p.shift) {
-					int sx = kx - p.ibtx, sy = y - p.ibty;
-					sx %= N; if (sx < 0) sx += N;
-					sy %= p.ny; if (sy < 0) sy += p.ny;
-					a = __ldg(p.wav0 + (long long)sy * N + sx);
-					const float cp = p.cppl ? __ldg(p.cppl + (long long)y * N + kx) : 0.f;
-					a = cmul(a, offset_factor(p.shift + 4 * b, kx, y, N, p.ny, cp));
-				}
-				else {
-					a = p.wav0 ? __ldg(p.wav0 + (long long)y * N + kx) : W[(long long)y * N + kx];
-				}
-				if (p.plane >= 0) readout_fourier(p, b, y, kx, a, acc);
-				v[m] = a;
+	int line, j;
+	T::template role<PL::T>(tid, line, j);
+	if (line < nval) {
+		const int y = row0 + line;
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) {
+			const int kx = j + PL::B * m;
+			float2 a;
+			if (p.shift) {
+				int sx = kx - p.ibtx, sy = y - p.ibty;
+				sx %= N; if (sx < 0) sx += N;
+				sy %= p.ny; if (sy < 0) sy += p.ny;
+				a = __ldg(p.wav0 + (long long)sy * N + sx);
+				const float cp = p.cppl ? __ldg(p.cppl + (long long)y * N + kx) : 0.f;
+				a = cmul(a, offset_factor(p.shift + 4 * b, kx, y, N, p.ny, cp));
 			}
+			else {
+				a = p.wav0 ? __ldg(p.wav0 + (long long)y * N + kx) : W[(long long)y * N + kx];
+			}
+			if (p.plane >= 0) readout_fourier(p, b, y, kx, a, acc);
+			v[m] = a;
 		}
 	}
 	if (p.plane >= 0 && p.ndet > 0) block_store_partials<NT>(acc, p, b);
-	line_fft<R1, R2, true, T>(v, sm, p.twx, tid, nval);
-	{
-		int line, k1;
-		T::template role<R1>(tid, line, k1);
-		if (line < nval) {
-			float2* dst = W + (long long)(row0 + line) * N;
-			#pragma unroll
-			for (int k2 = 0; k2 < R2; k2++) dst[k1 + R1 * k2] = v[k2];
-		}
+	PL::template to_mid<true, T>(v, sm, p.twx, tid);
+	int pos;
+	T::template role<PL::TMID>(tid, line, pos);
+	if (line < nval && pos < PL::TMID) {
+		float2* dst = W + (long long)(row0 + line) * N;
+		#pragma unroll
+		for (int e = 0; e < PL::EMID; e++) dst[PL::mid(pos, e)] = v[e];
 	}
 }
 
-// Row pass: FT_x -> x P -> Fourier readout (plane) -> IFT_x.
-template <int R1, int R2>
-__global__ void __launch_bounds__(row_lines<R1, R2>() * Geo<R1, R2>::RM)
+// Row pass: FT_x -> x P -> Fourier readout (plane) -> IFT_x.  READ selects
+// the variant with the readout code (used at readout planes only), so the
+// steps without readout do not carry its registers.
+template <class PL, bool READ>
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
 k_row_pass(const PassArgs p)
 {
-	constexpr int N = R1 * R2, RM = Geo<R1, R2>::RM, L = row_lines<R1, R2>(), NT = L * RM;
+	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
 	using T = RowTile<L>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
 	float2* W = p.work + (long long)b * p.wstride;
-	float2 v[RM];
-	{
-		int line, j;
-		T::template role<R2>(tid, line, j);
-		if (line < nval) {
-			const float2* src = W + (long long)(row0 + line) * N;
-			#pragma unroll
-			for (int m = 0; m < R1; m++) v[m] = src[j + R2 * m];
-		}
+	float2 v[PL::RM];
+	#pragma unroll
+	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
+	int line, j;
+	T::template role<PL::T>(tid, line, j);
+	if (line < nval) {
+		const float2* src = W + (long long)(row0 + line) * N;
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
-	line_fft<R1, R2, false, T>(v, sm, p.twx, tid, nval);
+	PL::template to_mid<false, T>(v, sm, p.twx, tid);
 	float acc[kMaxDet];
 	#pragma unroll
 	for (int d = 0; d < kMaxDet; d++) acc[d] = 0.f;
 	{
-		int line, k1;
-		T::template role<R1>(tid, line, k1);
-		if (line < nval) {
+		int pos;
+		T::template role<PL::TMID>(tid, line, pos);
+		if (line < nval && pos < PL::TMID) {
 			const int y = row0 + line;
 			const float2* P = p.mul + (long long)y * N;
 			#pragma unroll
-			for (int k2 = 0; k2 < R2; k2++) {
-				const int kx = k1 + R1 * k2;
-				v[k2] = cmul(v[k2], __ldg(P + kx));
-				if (p.plane >= 0) readout_fourier(p, b, y, kx, v[k2], acc);
+			for (int e = 0; e < PL::EMID; e++) {
+				const int kx = PL::mid(pos, e);
+				v[e] = cmul(v[e], __ldg(P + kx));
+				if (READ) readout_fourier(p, b, y, kx, v[e], acc);
 			}
 		}
 	}
-	if (p.plane >= 0 && p.ndet > 0) block_store_partials<NT>(acc, p, b);
+	if (READ && p.ndet > 0) block_store_partials<NT>(acc, p, b);
 	if (!p.store) return;
-	line_fft<R2, R1, true, T>(v, sm, p.twx, tid, nval);
-	{
-		int line, k;
-		T::template role<R2>(tid, line, k);
-		if (line < nval) {
-			float2* dst = W + (long long)(row0 + line) * N;
-			#pragma unroll
-			for (int k2 = 0; k2 < R1; k2++) dst[k + R2 * k2] = v[k2];
-		}
+	PL::template from_mid<true, T>(v, sm, p.twx, tid);
+	T::template role<PL::T>(tid, line, j);
+	if (line < nval) {
+		float2* dst = W + (long long)(row0 + line) * N;
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) dst[j + PL::B * m] = v[m];
 	}
 }
 
 // Column pass: IFT_y -> real-space readout (plane) -> x t -> FT_y.
-template <int R1, int R2>
-__global__ void __launch_bounds__(kColC * Geo<R1, R2>::RM)
+template <class PL, bool READ>
+__global__ void __launch_bounds__(kColC * PL::TMAX)
 k_col_pass(const PassArgs p)
 {
-	constexpr int N = R1 * R2, RM = Geo<R1, R2>::RM, C = kColC;
+	constexpr int C = kColC;
 	using T = ColTile<C>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
 	const int nval = min(C, p.nx - col0);
 	const int nx = p.nx;
 	float2* W = p.work + (long long)b * p.wstride + col0;
-	float2 v[RM];
-	{
-		int c, j;
-		T::template role<R2>(tid, c, j);
-		if (c < nval && j < R2) {
-			#pragma unroll
-			for (int m = 0; m < R1; m++) v[m] = W[(long long)(j + R2 * m) * nx + c];
-		}
+	float2 v[PL::RM];
+	#pragma unroll
+	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
+	int c, j;
+	T::template role<PL::T>(tid, c, j);
+	if (c < nval && j < PL::T) {
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) v[m] = W[(long long)(j + PL::B * m) * nx + c];
 	}
-	line_fft<R1, R2, true, T>(v, sm, p.twy, tid, nval);
+	PL::template to_mid<true, T>(v, sm, p.twy, tid);
 	{
-		int c, k1;
-		T::template role<R1>(tid, c, k1);
-		if (c < nval && k1 < R1) {
+		int pos;
+		T::template role<PL::TMID>(tid, c, pos);
+		if (c < nval && pos < PL::TMID) {
 			const int x = col0 + c;
 			const int xs = x % p.npgx;
 			#pragma unroll
-			for (int k2 = 0; k2 < R2; k2++) {
-				const int y = k1 + R1 * k2;
-				if (p.plane >= 0) readout_real(p, b, y, x, v[k2]);
-				v[k2] = cmul(v[k2], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
+			for (int e = 0; e < PL::EMID; e++) {
+				const int y = PL::mid(pos, e);
+				if (READ) readout_real(p, b, y, x, v[e]);
+				v[e] = cmul(v[e], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
 			}
 		}
 	}
-	line_fft<R2, R1, false, T>(v, sm, p.twy, tid, nval);
-	{
-		int c, k;
-		T::template role<R2>(tid, c, k);
-		if (c < nval && k < R2) {
-			#pragma unroll
-			for (int k2 = 0; k2 < R1; k2++) W[(long long)(k + R2 * k2) * nx + c] = v[k2];
-		}
+	PL::template from_mid<false, T>(v, sm, p.twy, tid);
+	T::template role<PL::T>(tid, c, j);
+	if (c < nval && j < PL::T) {
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) W[(long long)(j + PL::B * m) * nx + c] = v[m];
 	}
 }
 
 // Exit column pass: IFT_y -> real-space readout (plane), no store.
-template <int R1, int R2>
-__global__ void __launch_bounds__(kColC * Geo<R1, R2>::RM)
+template <class PL>
+__global__ void __launch_bounds__(kColC * PL::TMAX)
 k_exit_cols(const PassArgs p)
 {
-	constexpr int RM = Geo<R1, R2>::RM, C = kColC;
+	constexpr int C = kColC;
 	using T = ColTile<C>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
 	const int nval = min(C, p.nx - col0);
 	const int nx = p.nx;
 	const float2* W = p.work + (long long)b * p.wstride + col0;
-	float2 v[RM];
-	{
-		int c, j;
-		T::template role<R2>(tid, c, j);
-		if (c < nval && j < R2) {
-			#pragma unroll
-			for (int m = 0; m < R1; m++) v[m] = W[(long long)(j + R2 * m) * nx + c];
-		}
+	float2 v[PL::RM];
+	#pragma unroll
+	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
+	int c, j;
+	T::template role<PL::T>(tid, c, j);
+	if (c < nval && j < PL::T) {
+		#pragma unroll
+		for (int m = 0; m < PL::A; m++) v[m] = W[(long long)(j + PL::B * m) * nx + c];
 	}
-	line_fft<R1, R2, true, T>(v, sm, p.twy, tid, nval);
-	{
-		int c, k1;
-		T::template role<R1>(tid, c, k1);
-		if (c < nval && k1 < R1) {
-			#pragma unroll
-			for (int k2 = 0; k2 < R2; k2++) readout_real(p, b, k1 + R1 * k2, col0 + c, v[k2]);
-		}
+	PL::template to_mid<true, T>(v, sm, p.twy, tid);
+	int pos;
+	T::template role<PL::TMID>(tid, c, pos);
+	if (c < nval && pos < PL::TMID) {
+		#pragma unroll
+		for (int e = 0; e < PL::EMID; e++) readout_real(p, b, PL::mid(pos, e), col0 + c, v[e]);
 	}
 }
-
 
 // ---------------------------------------------------------------------------
 // launchers (explicitly instantiated per size in jms_inst_*.cu)
 // ---------------------------------------------------------------------------
-template <int R1, int R2>
-int row_smem_bytes()
-{
-	using T = RowTile<row_lines<R1, R2>()>;
-	int a = T::template sm_elems<R1, R2>(), b = T::template sm_elems<R2, R1>();
-	return (a > b ? a : b) * (int)sizeof(float2);
-}
-template <int R1, int R2>
-int col_smem_bytes()
-{
-	using T = ColTile<kColC>;
-	int a = T::template sm_elems<R1, R2>(), b = T::template sm_elems<R2, R1>();
-	return (a > b ? a : b) * (int)sizeof(float2);
-}
-
 template <class K>
 cudaError_t launch_k(K kern, dim3 grid, int threads, int smem, const PassArgs& p, cudaStream_t s)
 {
@@ -413,31 +523,41 @@ cudaError_t launch_k(K kern, dim3 grid, int threads, int smem, const PassArgs& p
 }
 
 template <int A, int B>
-int row_blocks_t(int ny) { return (ny + row_lines<A, B>() - 1) / row_lines<A, B>(); }
+int row_blocks_t(int ny) { using PL = Plan<A, B>; return (ny + row_lines<PL>() - 1) / row_lines<PL>(); }
 
 template <int A, int B>
 cudaError_t launch_entry_t(const PassArgs& p, cudaStream_t s)
 {
-	constexpr int L = row_lines<A, B>();
-	return launch_k(k_entry_rows<A, B>, dim3((p.ny + L - 1) / L, p.nwave), L * Geo<A, B>::RM, row_smem_bytes<A, B>(), p, s);
+	using PL = Plan<A, B>;
+	constexpr int L = row_lines<PL>();
+	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
+	return launch_k(k_entry_rows<PL>, dim3((p.ny + L - 1) / L, p.nwave), L * PL::TMAX, smem, p, s);
 }
 template <int A, int B>
 cudaError_t launch_row_t(const PassArgs& p, cudaStream_t s)
 {
-	constexpr int L = row_lines<A, B>();
-	return launch_k(k_row_pass<A, B>, dim3((p.ny + L - 1) / L, p.nwave), L * Geo<A, B>::RM, row_smem_bytes<A, B>(), p, s);
+	using PL = Plan<A, B>;
+	constexpr int L = row_lines<PL>();
+	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
+	const dim3 grid((p.ny + L - 1) / L, p.nwave);
+	if (p.plane >= 0) return launch_k(k_row_pass<PL, true>, grid, L * PL::TMAX, smem, p, s);
+	return launch_k(k_row_pass<PL, false>, grid, L * PL::TMAX, smem, p, s);
 }
 template <int A, int B>
 cudaError_t launch_col_t(const PassArgs& p, cudaStream_t s)
 {
-	return launch_k(k_col_pass<A, B>, dim3((p.nx + kColC - 1) / kColC, p.nwave), kColC * Geo<A, B>::RM,
-		col_smem_bytes<A, B>(), p, s);
+	using PL = Plan<A, B>;
+	constexpr int smem = PL::template smem_elems<ColTile<kColC>>() * (int)sizeof(float2);
+	const dim3 grid((p.nx + kColC - 1) / kColC, p.nwave);
+	if (p.plane >= 0) return launch_k(k_col_pass<PL, true>, grid, kColC * PL::TMAX, smem, p, s);
+	return launch_k(k_col_pass<PL, false>, grid, kColC * PL::TMAX, smem, p, s);
 }
 template <int A, int B>
 cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 {
-	return launch_k(k_exit_cols<A, B>, dim3((p.nx + kColC - 1) / kColC, p.nwave), kColC * Geo<A, B>::RM,
-		col_smem_bytes<A, B>(), p, s);
+	using PL = Plan<A, B>;
+	constexpr int smem = PL::template smem_elems<ColTile<kColC>>() * (int)sizeof(float2);
+	return launch_k(k_exit_cols<PL>, dim3((p.nx + kColC - 1) / kColC, p.nwave), kColC * PL::TMAX, smem, p, s);
 }
 
 #define JMS_INSTANTIATE(A, B) \
