@@ -336,7 +336,7 @@ def run_ours(args):
         if world == 1 and not args.no_cpu:
             try:
                 nt = host_threads()
-                sample = max(2 * nt, 8)
+                sample = 8 * nt
                 r, dt, _ = reference_cpu(cfg, sp, probe, pro, dets, pos, nt, sample)
                 line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": nt, "kind": "reference",
                                         "sample": f"{sample} probe positions x 1 phonon pass x 200 slices "
@@ -367,14 +367,16 @@ def traffic_from_profiles(kind):
 
 def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
     """Relative error of the integrated detector signals of one probe position
-    (one phonon pass, 200 slices) against the FP64 oracle."""
+    (one phonon pass, 200 slices) against the FP64 oracle, per detector (max
+    over the 11 readout planes, relative to that detector's largest signal),
+    next to the error of the reference's own FP32 CPU path on the same input."""
     try:
         from oracle import oracle as OR
     except Exception as ex:
         return {"det_rel": None, "sample": f"oracle unavailable: {ex}"}
     objslc = np.arange(cfg["nobj"]) % cfg["nslice_types"]
-    rng = OR.Rng(99)
-    var = rng.variant_sequence([cfg["nvar"]] * cfg["nslice_types"], objslc)
+    nvar = [cfg["nvar"]] * cfg["nslice_types"]
+    var = OR.Rng(99).variant_sequence(nvar, objslc)
     p = pos[len(pos) // 2:len(pos) // 2 + 1]
     e, out, _ = J.scan(p, 1, varseq=var[None, :])
     assert e == 0
@@ -384,10 +386,38 @@ def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
     res = OR.multislice(w0, np.concatenate(sp.gratings), objslc * cfg["nvar"] + var, pro[None],
                         np.zeros(cfg["nobj"], np.int32), hsh, n, det=np.stack([d for d, _ in dets]),
                         masks=[m for _, m in dets], imagedet=1)
-    ref = res["det_int"]
-    den = np.maximum(np.abs(ref).max(axis=0), 1e-30)
-    rel = float((np.abs(out[0] - ref).max(axis=0) / den).max())
-    return {"det_rel": rel, "sample": "1 position x 1 phonon pass x 200 slices, 11 planes x 3 detectors"}
+    ref_fp64 = res["det_int"]
+    den = np.maximum(np.abs(ref_fp64).max(axis=0), 1e-300)
+
+    def rel(x):
+        return [float(v) for v in np.abs(x - ref_fp64).max(axis=0) / den]
+
+    out_d = {"det_rel": rel(out[0]), "abs_vs_beam": float(np.abs(out[0] - ref_fp64).max()),
+             "signal_max": [float(v) for v in np.abs(ref_fp64).max(axis=0)],
+             "sample": "1 position x 1 phonon pass x 200 slices, 11 planes x 3 detectors; "
+                       "det_rel per detector (0-10, 20-50, 80-200 mrad)"}
+    try:  # the reference's own FP32 path (CPUMultislice on MKL) on the same input and variants
+        from oracle import ref
+        R = ref.RefJMS()
+        R.set_high_tension(cfg["kv"])
+        R.set_grid(cfg["nx"], cfg["ny"], sp.a, sp.b, 0.19525)
+        R.setup(ref.CODE_CPU, nvar, objslc, [0] * cfg["nslice_types"], cfg["ndetper"], len(dets), 1, 1)
+        for s_, gr in enumerate(sp.gratings):
+            R.set_phase_grating(ref.CODE_CPU, s_, gr)
+        R.set_propagator(ref.CODE_CPU, 0, pro)
+        for i, (d, m) in enumerate(dets):
+            R.set_detector(ref.CODE_CPU, i, d, m)
+        R.init_core(ref.CODE_CPU, 1)
+        R.set_incident_wave(ref.CODE_CPU, probe)
+        R.seed(99)
+        R.offset(ref.CODE_CPU, float(p[0, 0]), float(p[0, 1]), 0.0)
+        R.cpu_multislice(0, 0, 1.0, 0)
+        rd = R.get_result(ref.CODE_CPU, 1, n * len(dets)).reshape(n, len(dets))
+        R.close()
+        out_d["reference_fp32_det_rel"] = rel(rd)
+    except Exception as ex:
+        out_d["reference_fp32_det_rel"] = f"not run: {ex}"
+    return out_d
 
 
 def main():

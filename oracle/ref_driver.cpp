@@ -13,6 +13,7 @@
  */
 #include "JMultiSlice.h"
 #include <atomic>
+#include <dlfcn.h>
 #include <thread>
 #include <vector>
 #include <string>
@@ -120,7 +121,10 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	std::vector<std::thread> pool;
 	for (int t = 0; t < nthreads; t++) {
 		pool.emplace_back([&, t]() {
-			// MKL runs sequentially: the caller sets its global thread count to 1
+			// MKL runs sequentially in this worker: its OpenMP layer reads the
+			// thread count of the calling thread, which is set to 1 here
+			typedef void (*omp_set_t)(int);
+			if (omp_set_t f = (omp_set_t)dlsym(RTLD_DEFAULT, "omp_set_num_threads")) f(1);
 			RefJMS* jms = (RefJMS*)objs[t];
 			float w = 1.f / (float)nrepeat;
 			for (;;) {
