@@ -158,6 +158,24 @@ long long JMS_KernelLaunches(void);
  * summed milliseconds and launch counts since the last JMS_SetPassTiming. */
 void JMS_SetPassTiming(int on);
 int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row);
+/* Integrated detectors of caller-provided waves, allocating no memory.  No
+ * counterpart in the reference interface.  For callers that must not have
+ * the library allocate device memory while they run (a fixed memory pool
+ * owns the GPU, a real-time loop cannot afford the device synchronisation of
+ * cudaMalloc/cudaFree, or the footprint must stay fixed after start-up).
+ * d_wav: device, nwave Fourier-space waves [nwave][ny][nx] (interleaved
+ * float pairs, the grid of the current setup); d_out: device, double
+ * [nwave][ndet], overwritten with sum_k |psi(k)|^2 D_d(k) for the detectors
+ * of the current setup (masks applied).  stream: cudaStream_t or NULL for the
+ * library stream.  The per-CTA partial sums live in one fixed file-scope
+ * device array of 65536 floats (256 KiB per GPU, held until the process
+ * ends); calls needing more than nwave * ndet * ceil(ny / 8) <= 65536 are
+ * refused with 131.  All calls share that array, so calls that overlap on
+ * the GPU race.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress) with that device current: make it before any stream
+ * capture.  Returns 0, 1 (bad arguments), 2 (setup incomplete), 131, 132
+ * (address lookup failed) or 133 (launch failed). */
+int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream);
 /* 1 if both grid lengths are supported by the fused passes. */
 int JMS_GridSupported(int nx, int ny);
 

@@ -69,6 +69,7 @@ SIGNATURES = {
     "JMS_ScanGPUDevice": ([_i, _p, _f, _i, _ip, _p, _p, _i], _i),
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
+    "JMS_ReadoutDetectorsNoAlloc": ([_p, _i, _p, _p], _i),
     "JMS_SetPassTiming": ([_i], None),
     "JMS_PassTiming": ([_dp, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong)], _i),
 }

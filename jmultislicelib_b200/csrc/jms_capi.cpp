@@ -147,6 +147,8 @@ long long JMS_KernelLaunches(void) { return J().KernelLaunches(); }
 void JMS_SetPassTiming(int on) { J().SetPassTiming(on); }
 int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row)
 { return J().PassTiming(ms_col, n_col, ms_row, n_row); }
+int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream)
+{ return J().ReadoutDetectorsNoAlloc(d_wav, nwave, d_out, (cudaStream_t)stream); }
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
 
 } // extern "C"

@@ -815,6 +815,19 @@ int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, co
 	return 0;
 }
 
+int JmsB200::ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, cudaStream_t s)
+{
+	if (d_wav == nullptr || d_out == nullptr || nwave < 1) return 1;
+	if (!(status_gpu_ & STATUS_DET) || !(status_gpu_ & STATUS_CORE) || d_det_ == nullptr || ndet_ < 1) return 2;
+	const int e = launch_readout_noalloc((const float2*)d_wav, nwave, nx_, ny_, d_det_, ndet_, d_out,
+		s ? s : stream_);
+	if (e == 131)
+		std::fprintf(stderr, "Error: (ReadoutDetectorsNoAlloc): %d waves x %d detectors need more than the %d "
+			"partial sums of the fixed scratch array.\n", nwave, ndet_, noalloc_capacity());
+	if (e == 0) launches_ += 2;
+	return e;
+}
+
 int JmsB200::ScanGPU(int npos, const float* pos, float dz, int npass, const int* varseq, float* out_int,
 	float* out_bin, int bin)
 {

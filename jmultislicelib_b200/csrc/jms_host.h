@@ -123,6 +123,10 @@ public:
 	// the library stream).  out_int is double [npos][ndetslc][ndet].
 	int ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const int* varseq, double* d_out_int,
 		float* d_out_bin, int bin);
+	// Integrated detectors of caller-provided Fourier-space waves (device
+	// pointers) with the current detector setup, allocating nothing
+	// (jms_noalloc.cu); d_out is double [nwave][ndet], overwritten.
+	int ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, cudaStream_t s);
 	int SetScanBatch(int nwave) { scan_batch_ = nwave > 0 ? nwave : scan_batch_; return 0; }
 	int GetScanBatch() const { return scan_batch_; }
 	long long KernelLaunches() const { return launches_; }

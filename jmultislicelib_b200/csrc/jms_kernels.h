@@ -79,6 +79,15 @@ cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int nd
 cudaError_t launch_make_shift(double* d_shift, const float* d_pos, int npos, double a, double b, double fz,
 	cudaStream_t s);
 
+// Integrated-detector readout of nwave Fourier-space waves [nwave][ny][nx]
+// that allocates nothing: its partial sums live in a fixed file-scope device
+// array (jms_noalloc.cu).  out[w][d] = sum_k |wav_w(k)|^2 det_d(k) (FP64,
+// overwritten).  Returns 0, 131 (needs more than noalloc_capacity() partial
+// sums), 132 (no device address for the array) or 133 (launch error).
+int launch_readout_noalloc(const float2* wav, int nwave, int nx, int ny, const float* det, int ndet, double* out,
+	cudaStream_t s);
+int noalloc_capacity();
+
 // drop-in OffsetIncomingWave: out = wav0(k - tilt) * exp(-i(2 pi turns + cppl))
 cudaError_t launch_offset(float2* out, const float2* wav0, int nx, int ny, const double* shift_host4,
 	const float* cppl, int ibtx, int ibty, cudaStream_t s);
