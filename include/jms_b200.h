@@ -176,6 +176,18 @@ int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* 
  * capture.  Returns 0, 1 (bad arguments), 2 (setup incomplete), 131, 132
  * (address lookup failed) or 133 (launch failed). */
 int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream);
+/* Line-plan autotuner (no counterpart in the reference): times each candidate
+ * FFT plan of nx (row passes) and ny (column passes) on nwave waves of the
+ * current setup (reps launches each, CUDA events) and keeps the fastest for
+ * this and later setups of the same lengths in the process.  Outputs (may be
+ * NULL): average ms per launch of the chosen plans and their indices. */
+int JMS_Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* irow, int* icol);
+/* Chooses the row / column plans by index (0 = default); 1 if out of range. */
+int JMS_SelectPlans(int irow, int icol);
+/* Number of candidate plans for line length n (0 = length not supported). */
+int JMS_PlanCount(int n);
+/* Name of the plan in use for axis 0 (rows, nx) or 1 (columns, ny). */
+int JMS_PlanName(int axis, char* name, int len);
 /* 1 if both grid lengths are supported by the fused passes. */
 int JMS_GridSupported(int nx, int ny);
 

@@ -70,6 +70,10 @@ SIGNATURES = {
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
     "JMS_ReadoutDetectorsNoAlloc": ([_p, _i, _p, _p], _i),
+    "JMS_Autotune": ([_i, _i, _fp, _fp, _ip, _ip], _i),
+    "JMS_SelectPlans": ([_i, _i], _i),
+    "JMS_PlanCount": ([_i], _i),
+    "JMS_PlanName": ([_i, C.c_char_p, _i], _i),
     "JMS_SetPassTiming": ([_i], None),
     "JMS_PassTiming": ([_dp, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong)], _i),
 }

@@ -149,6 +149,17 @@ int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* 
 { return J().PassTiming(ms_col, n_col, ms_row, n_row); }
 int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream)
 { return J().ReadoutDetectorsNoAlloc(d_wav, nwave, d_out, (cudaStream_t)stream); }
+int JMS_Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* irow, int* icol)
+{ return J().Autotune(nwave, reps, ms_row, ms_col, irow, icol); }
+int JMS_SelectPlans(int irow, int icol) { return J().SelectPlans(irow, icol); }
+int JMS_PlanCount(int n) { return jms::plan_count(n); }
+int JMS_PlanName(int axis, char* name, int len)
+{
+	if (!name || len < 1) return 1;
+	std::strncpy(name, J().PlanName(axis), (size_t)len - 1);
+	name[len - 1] = 0;
+	return 0;
+}
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
 
 } // extern "C"

@@ -23,6 +23,8 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <map>
+#include <mutex>
 
 namespace jms {
 
@@ -32,6 +34,17 @@ void dfree(T*& p)
 {
 	if (p) cudaFree((void*)p);
 	p = nullptr;
+}
+
+// plan choices made by Autotune in this process: (length, axis) -> index
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int> g_tuned;
+
+int tuned_plan(int n, int axis)
+{
+	std::lock_guard<std::mutex> lock(g_tune_mu);
+	auto it = g_tuned.find({n, axis});
+	return it == g_tuned.end() ? 0 : it->second;
 }
 } // namespace
 
@@ -363,6 +376,10 @@ int JmsB200::InitCore(int whichcode, int)
 			std::fprintf(stderr, "Error: (InitCore): grid %d x %d not supported by the fused passes.\n", nx_, ny_);
 			return 103;
 		}
+		prow_ = plan_get(nx_, tuned_plan(nx_, 0));
+		pcol_ = plan_get(ny_, tuned_plan(ny_, 1));
+		if (!prow_) prow_ = plan_get(nx_, 0);
+		if (!pcol_) pcol_ = plan_get(ny_, 0);
 		if (!stream_) {
 			if (post(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "InitCore")) return 103;
 			own_stream_ = true;
@@ -514,7 +531,7 @@ int JmsB200::ensure_work(int nwave)
 
 int JmsB200::ensure_partial(int nwave)
 {
-	const int nblk = row_blocks_per_wave(nx_, ny_);
+	const int nblk = prow_ ? prow_->row_blocks(ny_) : 1;
 	const size_t need = (size_t)std::max(1, nwave) * std::max(1, ndetslc_) * std::max(1, ndet_) * std::max(1, nblk);
 	if (need <= partial_cap_ && d_partial_) return 0;
 	dfree(d_partial_);
@@ -532,6 +549,7 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 	const double* d_shift, int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx,
 	int nby)
 {
+	if (!prow_ || !pcol_) return 2;
 	if (ensure_work(nwave) || ensure_partial(nwave)) return 1;
 	const long long N = (long long)nx_ * ny_;
 	const bool b_dif = (imagedet_ & (DET_INTEGRATED | DET_DIFFRACTION | DET_WAVEFOURIER | DET_DIFFR_AVG | DET_WAVEF_AVG)) != 0;
@@ -551,7 +569,7 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 	base.ndet = (ndet > 0 && d_detint) ? ndet : 0;
 	base.det = d_det_;
 	base.partial = d_partial_;
-	base.nblk = row_blocks_per_wave(nx_, ny_);
+	base.nblk = prow_->row_blocks(ny_);
 	base.chan_wstride = 0;
 	base.bin_out = d_bin;
 	base.bin = bin > 0 ? bin : 1;
@@ -579,7 +597,7 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		p.ibtx = ibtx;
 		p.ibty = ibty;
 		p.plane = b_dif ? plane_of(islc) : -1;
-		if (post(launch_entry_rows(p, s), "GPUMultislice entry")) return 101;
+		if (post(prow_->entry(p, s), "GPUMultislice entry")) return 101;
 		launches_++;
 	}
 	for (int j = islc; j < nobjslc_; j++) {
@@ -590,21 +608,21 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		c.npgy = npgy_;
 		c.plane = b_img ? plane_of(j) : -1;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
-		if (post(launch_col_pass(c, s), "GPUMultislice column pass")) return 401;
+		if (post(pcol_->col(c, s), "GPUMultislice column pass")) return 401;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
 		PassArgs r = four;
 		r.mul = d_pro_ + (long long)proidx_[st] * N;
 		r.plane = b_dif ? plane_of(j + 1) : -1;
 		r.store = (j + 1 < nobjslc_ || b_img) ? 1 : 0;
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
-		if (post(launch_row_pass(r, s), "GPUMultislice row pass")) return 601;
+		if (post(prow_->row(r, s), "GPUMultislice row pass")) return 601;
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
 		launches_ += 2;
 	}
 	if (b_img) { // exit plane image readout
 		PassArgs c = real;
 		c.plane = plane_of(nobjslc_);
-		if (post(launch_exit_cols(c, s), "GPUMultislice exit image")) return 901;
+		if (post(pcol_->exit(c, s), "GPUMultislice exit image")) return 901;
 		launches_++;
 	}
 	if (base.ndet > 0) {
@@ -753,6 +771,84 @@ int JmsB200::PassTiming(double* ms_col, long long* n_col, double* ms_row, long l
 	};
 	sum(ev_col_, ms_col, n_col);
 	sum(ev_row_, ms_row, n_row);
+	return 0;
+}
+
+int JmsB200::SelectPlans(int irow, int icol)
+{
+	const PlanOps* r = plan_get(nx_, irow);
+	const PlanOps* c = plan_get(ny_, icol);
+	if (!r || !c) return 1;
+	prow_ = r;
+	pcol_ = c;
+	return 0;
+}
+
+const char* JmsB200::PlanName(int axis) const
+{
+	const PlanOps* p = axis == 0 ? prow_ : pcol_;
+	return p ? p->name : "";
+}
+
+// Times reps launches of every candidate row plan (propagator 0, no readout)
+// and column plan (first grating, no readout) on nwave waves of the current
+// setup, with CUDA events on the library stream, and keeps the fastest.
+int JmsB200::Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* irow, int* icol)
+{
+	if (!(status_gpu_ & STATUS_CORE) || !d_pro_ || !d_pgr_ || nwave < 1 || reps < 1) return 2;
+	if (ensure_work(nwave)) return 1;
+	cudaStream_t s = stream_;
+	cudaMemsetAsync(d_work_, 0, sizeof(float2) * (size_t)nwave * nx_ * ny_, s);
+	PassArgs base;
+	base.work = d_work_;
+	base.wstride = (long long)nx_ * ny_;
+	base.nx = nx_;
+	base.ny = ny_;
+	base.nwave = nwave;
+	base.twx = d_twx_;
+	base.twy = d_twy_;
+	base.npgx = npgx_;
+	base.npgy = npgy_;
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	auto time_it = [&](cudaError_t (*fn)(const PassArgs&, cudaStream_t), const PassArgs& p) -> float {
+		if (fn(p, s) != cudaSuccess) return 1e30f;            // warm-up launch (also sets attributes)
+		cudaEventRecord(e0, s);
+		for (int k = 0; k < reps; k++) fn(p, s);
+		cudaEventRecord(e1, s);
+		if (cudaEventSynchronize(e1) != cudaSuccess) return 1e30f;
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, e0, e1);
+		return ms / reps;
+	};
+	int best_r = 0, best_c = 0;
+	float tr = 1e30f, tc = 1e30f;
+	for (int i = 0; i < plan_count(nx_); i++) {
+		PassArgs p = base;
+		p.mul = d_pro_;
+		const float t = time_it(plan_get(nx_, i)->row, p);
+		if (t < tr) { tr = t; best_r = i; }
+	}
+	for (int i = 0; i < plan_count(ny_); i++) {
+		PassArgs p = base;
+		p.mul = d_pgr_;
+		const float t = time_it(plan_get(ny_, i)->col, p);
+		if (t < tc) { tc = t; best_c = i; }
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (post(cudaGetLastError(), "Autotune")) return 3;
+	{
+		std::lock_guard<std::mutex> lock(g_tune_mu);
+		g_tuned[{nx_, 0}] = best_r;
+		g_tuned[{ny_, 1}] = best_c;
+	}
+	SelectPlans(best_r, best_c);
+	if (ms_row) *ms_row = tr;
+	if (ms_col) *ms_col = tc;
+	if (irow) *irow = best_r;
+	if (icol) *icol = best_c;
 	return 0;
 }
 

@@ -18,6 +18,8 @@
 
 namespace jms {
 
+struct PlanOps;
+
 // flags (numeric values of src/JMultiSlice.h:126-149)
 enum : int {
 	CODE_CPU = 1, CODE_GPU = 2,
@@ -128,6 +130,13 @@ public:
 	// (jms_noalloc.cu); d_out is double [nwave][ndet], overwritten.
 	int ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, cudaStream_t s);
 	int SetScanBatch(int nwave) { scan_batch_ = nwave > 0 ? nwave : scan_batch_; return 0; }
+	// Line-plan choice (jms_sizes.h): Autotune times every candidate plan of
+	// nx (row passes) and ny (column passes) on nwave waves of the current
+	// setup and keeps the fastest; the choice is remembered per length for
+	// later setups in this process.  SelectPlans sets them by index.
+	int Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* irow, int* icol);
+	int SelectPlans(int irow, int icol);
+	const char* PlanName(int axis) const;
 	int GetScanBatch() const { return scan_batch_; }
 	long long KernelLaunches() const { return launches_; }
 	// Per-pass device timing: with it on, every column / row pass launch is
@@ -184,6 +193,8 @@ private:
 	int scan_batch_ = 32;
 	int descan_on_ = 0, descan_x_ = 0, descan_y_ = 0;
 	int timing_on_ = 0;
+	const PlanOps* prow_ = nullptr;  // plan of the row / entry passes (length nx)
+	const PlanOps* pcol_ = nullptr;  // plan of the column / exit passes (length ny)
 	std::vector<cudaEvent_t> ev_col_, ev_row_;   // start/stop pairs
 	cudaEvent_t timed_event();
 	int plasmon_on_ = 0;

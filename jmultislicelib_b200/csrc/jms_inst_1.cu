@@ -1,10 +1,12 @@
-// jms_inst_1.cu -- pass instantiations for line lengths 120, 128, 160, 192, 240.
+// jms_inst_1.cu -- pass instantiations for plans P120, P128a, P128b, P160, P192, P240.
 #include "jms_passes.cuh"
+#include "jms_sizes.h"
 
 namespace jms {
-JMS_INSTANTIATE(10, 12)
-JMS_INSTANTIATE(8, 16)
-JMS_INSTANTIATE(10, 16)
-JMS_INSTANTIATE(12, 16)
-JMS_INSTANTIATE(15, 16)
+JMS_INSTANTIATE(P120)
+JMS_INSTANTIATE(P128a)
+JMS_INSTANTIATE(P128b)
+JMS_INSTANTIATE(P160)
+JMS_INSTANTIATE(P192)
+JMS_INSTANTIATE(P240)
 } // namespace jms

@@ -1,7 +1,8 @@
-// jms_inst_3.cu -- pass instantiations for line lengths 480, 512.
+// jms_inst_3.cu -- pass instantiations for plans P480, P512a.
 #include "jms_passes.cuh"
+#include "jms_sizes.h"
 
 namespace jms {
-JMS_INSTANTIATE(20, 24)
-JMS_INSTANTIATE(16, 32)
+JMS_INSTANTIATE(P480)
+JMS_INSTANTIATE(P512a)
 } // namespace jms

@@ -1,7 +1,8 @@
-// jms_inst_5.cu -- pass instantiations for line lengths 768, 960.
+// jms_inst_5.cu -- pass instantiations for plans P640, P720.
 #include "jms_passes.cuh"
+#include "jms_sizes.h"
 
 namespace jms {
-JMS_INSTANTIATE(24, 32)
-JMS_INSTANTIATE(30, 32)
+JMS_INSTANTIATE(P640)
+JMS_INSTANTIATE(P720)
 } // namespace jms

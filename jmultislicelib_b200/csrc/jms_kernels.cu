@@ -54,42 +54,29 @@ __global__ void k_offset(float2* out, const float2* __restrict__ wav0, int nx, i
 
 
 // ---------------------------------------------------------------------------
-// dispatch over supported line lengths
+// plan table
 // ---------------------------------------------------------------------------
-bool pass_supported(int n)
-{
-	switch (n) {
-#define X(n_, a_, b_) case n_: return true;
-		JMS_SIZES(X)
+static const PlanOps kPlans[] = {
+#define X(n_, pl_, name_) {n_, name_, &row_blocks_t<pl_>, &launch_entry_t<pl_>, &launch_row_t<pl_>, \
+	&launch_col_t<pl_>, &launch_exit_t<pl_>},
+	JMS_PLANS(X)
 #undef X
-	default: return false;
-	}
+};
+static constexpr int kNumPlans = (int)(sizeof(kPlans) / sizeof(kPlans[0]));
+
+int plan_count(int n)
+{
+	int c = 0;
+	for (int i = 0; i < kNumPlans; i++) c += (kPlans[i].n == n);
+	return c;
 }
 
-int row_blocks_per_wave(int nx, int ny)
+const PlanOps* plan_get(int n, int idx)
 {
-	switch (nx) {
-#define X(n_, a_, b_) case n_: return row_blocks_t<a_, b_>(ny);
-		JMS_SIZES(X)
-#undef X
-	default: return 0;
-	}
+	for (int i = 0; i < kNumPlans; i++)
+		if (kPlans[i].n == n && idx-- == 0) return &kPlans[i];
+	return nullptr;
 }
-
-#define JMS_DISPATCH(fn, len) \
-	switch (len) { \
-	JMS_SIZES(JMS_CASE_##fn) \
-	default: return cudaErrorInvalidValue; \
-	}
-#define JMS_CASE_entry(n_, a_, b_) case n_: return launch_entry_t<a_, b_>(p, s);
-#define JMS_CASE_row(n_, a_, b_) case n_: return launch_row_t<a_, b_>(p, s);
-#define JMS_CASE_col(n_, a_, b_) case n_: return launch_col_t<a_, b_>(p, s);
-#define JMS_CASE_exit(n_, a_, b_) case n_: return launch_exit_t<a_, b_>(p, s);
-
-cudaError_t launch_entry_rows(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(entry, p.nx) }
-cudaError_t launch_row_pass(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(row, p.nx) }
-cudaError_t launch_col_pass(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(col, p.ny) }
-cudaError_t launch_exit_cols(const PassArgs& p, cudaStream_t s) { JMS_DISPATCH(exit, p.ny) }
 
 cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
 	double* det_int, cudaStream_t s)

@@ -61,15 +61,21 @@ struct PassArgs {
 	int ibtx = 0, ibty = 0;         // beam tilt in Fourier pixels
 };
 
-// Supported line lengths: products of two factors <= 32 built from 2, 3, 5.
-bool pass_supported(int n);
-
-// launchers (return cudaSuccess or the launch error)
-cudaError_t launch_entry_rows(const PassArgs& p, cudaStream_t s);
-cudaError_t launch_row_pass(const PassArgs& p, cudaStream_t s);
-cudaError_t launch_col_pass(const PassArgs& p, cudaStream_t s);
-cudaError_t launch_exit_cols(const PassArgs& p, cudaStream_t s);
-int row_blocks_per_wave(int nx, int ny);
+// Line plans: every supported length n has one or more candidate plans
+// (jms_sizes.h); the row/entry passes use the plan chosen for nx, the
+// column/exit passes the plan chosen for ny.  Index 0 is a length's default.
+struct PlanOps {
+	int n;
+	const char* name;
+	int (*row_blocks)(int ny);                              // row-pass CTAs per wave
+	cudaError_t (*entry)(const PassArgs&, cudaStream_t);    // entry row pass
+	cudaError_t (*row)(const PassArgs&, cudaStream_t);      // row pass
+	cudaError_t (*col)(const PassArgs&, cudaStream_t);      // column pass
+	cudaError_t (*exit)(const PassArgs&, cudaStream_t);     // exit column pass
+};
+int plan_count(int n);
+const PlanOps* plan_get(int n, int idx);
+inline bool pass_supported(int n) { return plan_count(n) > 0; }
 
 // det_int[w][plane][d] += weight * sum_blk partial[w][plane][d][blk] (FP64)
 cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,

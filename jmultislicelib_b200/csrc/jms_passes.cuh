@@ -53,6 +53,30 @@ struct RowTile {
 	__device__ __forceinline__ static int s_inv(int line, int q2, int n1) { return (line * A + n1) * (B + 2) + q2; }
 	template <int A, int B>
 	static constexpr int sm_split() { return LINES * A * (B + 2); }
+	// 3-stage exchanges for N = R^3 (see fft3): S1(line, k1, t) and
+	// S2(line, k1, k2, j) in separate regions; the strides make the 16 lanes
+	// of a half warp (k1 = t mod R fastest) hit distinct bank pairs
+	template <int R>
+	__host__ __device__ static constexpr int s3a_row() { return R * R + ((16 / R - R * R) % 16 + 16) % 16; }   // = 16/R mod 16
+	template <int R>
+	__host__ __device__ static constexpr int s3b_j() { return R + ((1 - R) % 16 + 16) % 16; }                    // = 1 mod 16
+	template <int R>
+	__host__ __device__ static constexpr int s3b_k1()
+	{
+		constexpr int base = R * s3b_j<R>();
+		return base + ((16 / R - base) % 16 + 16) % 16;                                          // = 16/R mod 16
+	}
+	template <int R>
+	__host__ __device__ static constexpr int s3_line() { return R * s3a_row<R>() + R * s3b_k1<R>(); }
+	template <int R>
+	__device__ __forceinline__ static int s3a(int line, int k1, int t) { return line * s3_line<R>() + k1 * s3a_row<R>() + t; }
+	template <int R>
+	__device__ __forceinline__ static int s3b(int line, int k1, int k2, int j)
+	{
+		return line * s3_line<R>() + R * s3a_row<R>() + k1 * s3b_k1<R>() + k2 * s3b_j<R>() + j;
+	}
+	template <int R>
+	static constexpr int sm3() { return LINES * s3_line<R>(); }
 };
 
 // Column tile: C columns per CTA; thread t -> (column t % C, position t / C),
@@ -76,6 +100,16 @@ struct ColTile {
 	__device__ __forceinline__ static int s_inv(int line, int q2, int n1) { return n1 * (B * C + PAD) + q2 * C + line; }
 	template <int A, int B>
 	static constexpr int sm_split() { return A * (B * C + PAD); }
+	// 3-stage exchanges: S1(c, k1, t) then S2(c, k1, k2, j), column fastest
+	template <int R>
+	__device__ __forceinline__ static int s3a(int line, int k1, int t) { return k1 * (R * R * C + PAD) + t * C + line; }
+	template <int R>
+	__device__ __forceinline__ static int s3b(int line, int k1, int k2, int j)
+	{
+		return R * (R * R * C + PAD) + k1 * (R * R * C + PAD) + (k2 * R + j) * C + line;
+	}
+	template <int R>
+	static constexpr int sm3() { return 2 * R * (R * R * C + PAD); }
 };
 
 // twiddle by table value w = exp(-2 pi i k / N) (conjugated for the inverse)
@@ -180,8 +214,42 @@ __device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const fl
 	__syncthreads();
 }
 
+// ---- 3 stages, N = R^3 ---------------------------------------------------------
+// T = R^2 threads per line; thread t holds x[t + T m] (m < R) on entry and
+// X[t + T k3] (k3 < R) on exit, so the transform maps its layout onto itself.
+//   stage A: R-point DFT over m, twiddle W_N^(t k1), exchange S1;
+//   stage B: thread (k1 = t mod R, j = t / R) takes Y[k1][j + R m'], R-point
+//            DFT over m', twiddle W_N^(R j k2), exchange S2;
+//   stage C: thread (k1, k2 = t / R) takes the R values over j, R-point DFT.
+// S1 and S2 are separate regions, so two barriers per transform suffice.
+template <int R, bool INV, class Tile, int RM>
+__device__ __forceinline__ void fft3(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+{
+	constexpr int T = R * R;
+	int line, t;
+	Tile::template role<T>(tid, line, t);
+	dft_reg<R, 1, 0, INV>(v);
+	#pragma unroll
+	for (int k1 = 1; k1 < R; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + t * k1));
+	#pragma unroll
+	for (int k1 = 0; k1 < R; k1++) sm[Tile::template s3a<R>(line, k1, t)] = v[k1];
+	__syncthreads();
+	const int k1 = t % R, jj = t / R;
+	#pragma unroll
+	for (int m = 0; m < R; m++) v[m] = sm[Tile::template s3a<R>(line, k1, jj + R * m)];
+	dft_reg<R, 1, 0, INV>(v);
+	#pragma unroll
+	for (int k2 = 1; k2 < R; k2++) v[k2] = tw_mul<INV>(v[k2], __ldg(tw + R * jj * k2));
+	#pragma unroll
+	for (int k2 = 0; k2 < R; k2++) sm[Tile::template s3b<R>(line, k1, k2, jj)] = v[k2];
+	__syncthreads();
+	#pragma unroll
+	for (int j = 0; j < R; j++) v[j] = sm[Tile::template s3b<R>(line, k1, jj, j)];
+	dft_reg<R, 1, 0, INV>(v);
+}
+
 // ---- plans -------------------------------------------------------------------------
-template <int A_, int B_>
+template <int A_, int B_, int CC_ = 16>
 struct Plan {
 	static constexpr int A = A_, B = B_, N = A_ * B_;
 	static constexpr int S = (B_ == 2 * A_ && A_ >= 4) ? 2 : 1;
@@ -190,6 +258,7 @@ struct Plan {
 	static constexpr int TMID = (S == 2) ? B_ : A_;                    // threads per line (middle layout)
 	static constexpr int EMID = (S == 2) ? A_ : B_;                    // values per thread (middle layout)
 	static constexpr int TMAX = (T > TMID) ? T : TMID;
+	static constexpr int CC = CC_;                                     // columns per column-pass CTA
 	// line index of the e-th middle value of position pos
 	__device__ __forceinline__ static int mid(int pos, int e)
 	{
@@ -219,6 +288,31 @@ struct Plan {
 	}
 };
 
+// Three equal radices: N = R^3, R^2 threads per line with R values each; the
+// middle layout equals the load layout.
+template <int R_, int CC_ = 8>
+struct Plan3 {
+	static constexpr int R = R_, N = R_ * R_ * R_;
+	static constexpr int A = R_, B = R_ * R_;            // load layout: thread j holds x[j + B m], m < A
+	static constexpr int RM = R_, T = B, TMID = B, EMID = R_, TMAX = B;
+	static constexpr int CC = CC_;
+	__device__ __forceinline__ static int mid(int pos, int e) { return pos + B * e; }
+	template <bool INV, class Tile>
+	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	{
+		fft3<R_, INV, Tile>(v, sm, tw, tid);
+	}
+	template <bool INV, class Tile>
+	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	{
+		// the second transform writes S1 before its first barrier; the barriers
+		// of the first transform already ordered all reads of S1 before it
+		fft3<R_, INV, Tile>(v, sm, tw, tid);
+	}
+	template <class Tile>
+	static constexpr int smem_elems() { return Tile::template sm3<R_>(); }
+};
+
 __host__ __device__ constexpr int gcd_ct(int a, int b) { return b == 0 ? a : gcd_ct(b, a % b); }
 // rows per row-pass CTA: about 256 threads, a whole number of warps
 template <class PL>
@@ -229,7 +323,6 @@ __host__ __device__ constexpr int row_lines()
 	constexpr int l = (256 / T) / m * m;
 	return l < m ? m : l;
 }
-constexpr int kColC = 16;
 
 // ---------------------------------------------------------------------------
 // readouts
@@ -435,10 +528,10 @@ k_row_pass(const PassArgs p)
 
 // Column pass: IFT_y -> real-space readout (plane) -> x t -> FT_y.
 template <class PL, bool READ>
-__global__ void __launch_bounds__(kColC * PL::TMAX)
+__global__ void __launch_bounds__(PL::CC * PL::TMAX)
 k_col_pass(const PassArgs p)
 {
-	constexpr int C = kColC;
+	constexpr int C = PL::CC;
 	using T = ColTile<C>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
@@ -479,10 +572,10 @@ k_col_pass(const PassArgs p)
 
 // Exit column pass: IFT_y -> real-space readout (plane), no store.
 template <class PL>
-__global__ void __launch_bounds__(kColC * PL::TMAX)
+__global__ void __launch_bounds__(PL::CC * PL::TMAX)
 k_exit_cols(const PassArgs p)
 {
-	constexpr int C = kColC;
+	constexpr int C = PL::CC;
 	using T = ColTile<C>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
@@ -522,49 +615,47 @@ cudaError_t launch_k(K kern, dim3 grid, int threads, int smem, const PassArgs& p
 	return cudaGetLastError();
 }
 
-template <int A, int B>
-int row_blocks_t(int ny) { using PL = Plan<A, B>; return (ny + row_lines<PL>() - 1) / row_lines<PL>(); }
+template <class PL>
+int row_blocks_t(int ny) { return (ny + row_lines<PL>() - 1) / row_lines<PL>(); }
 
-template <int A, int B>
+template <class PL>
 cudaError_t launch_entry_t(const PassArgs& p, cudaStream_t s)
 {
-	using PL = Plan<A, B>;
 	constexpr int L = row_lines<PL>();
 	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
 	return launch_k(k_entry_rows<PL>, dim3((p.ny + L - 1) / L, p.nwave), L * PL::TMAX, smem, p, s);
 }
-template <int A, int B>
+template <class PL>
 cudaError_t launch_row_t(const PassArgs& p, cudaStream_t s)
 {
-	using PL = Plan<A, B>;
 	constexpr int L = row_lines<PL>();
 	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
 	const dim3 grid((p.ny + L - 1) / L, p.nwave);
 	if (p.plane >= 0) return launch_k(k_row_pass<PL, true>, grid, L * PL::TMAX, smem, p, s);
 	return launch_k(k_row_pass<PL, false>, grid, L * PL::TMAX, smem, p, s);
 }
-template <int A, int B>
+template <class PL>
 cudaError_t launch_col_t(const PassArgs& p, cudaStream_t s)
 {
-	using PL = Plan<A, B>;
-	constexpr int smem = PL::template smem_elems<ColTile<kColC>>() * (int)sizeof(float2);
-	const dim3 grid((p.nx + kColC - 1) / kColC, p.nwave);
-	if (p.plane >= 0) return launch_k(k_col_pass<PL, true>, grid, kColC * PL::TMAX, smem, p, s);
-	return launch_k(k_col_pass<PL, false>, grid, kColC * PL::TMAX, smem, p, s);
+	constexpr int C = PL::CC;
+	constexpr int smem = PL::template smem_elems<ColTile<C>>() * (int)sizeof(float2);
+	const dim3 grid((p.nx + C - 1) / C, p.nwave);
+	if (p.plane >= 0) return launch_k(k_col_pass<PL, true>, grid, C * PL::TMAX, smem, p, s);
+	return launch_k(k_col_pass<PL, false>, grid, C * PL::TMAX, smem, p, s);
 }
-template <int A, int B>
+template <class PL>
 cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 {
-	using PL = Plan<A, B>;
-	constexpr int smem = PL::template smem_elems<ColTile<kColC>>() * (int)sizeof(float2);
-	return launch_k(k_exit_cols<PL>, dim3((p.nx + kColC - 1) / kColC, p.nwave), kColC * PL::TMAX, smem, p, s);
+	constexpr int C = PL::CC;
+	constexpr int smem = PL::template smem_elems<ColTile<C>>() * (int)sizeof(float2);
+	return launch_k(k_exit_cols<PL>, dim3((p.nx + C - 1) / C, p.nwave), C * PL::TMAX, smem, p, s);
 }
 
-#define JMS_INSTANTIATE(A, B) \
-	template int row_blocks_t<A, B>(int); \
-	template cudaError_t launch_entry_t<A, B>(const PassArgs&, cudaStream_t); \
-	template cudaError_t launch_row_t<A, B>(const PassArgs&, cudaStream_t); \
-	template cudaError_t launch_col_t<A, B>(const PassArgs&, cudaStream_t); \
-	template cudaError_t launch_exit_t<A, B>(const PassArgs&, cudaStream_t);
+#define JMS_INSTANTIATE(PL) \
+	template int row_blocks_t<PL>(int); \
+	template cudaError_t launch_entry_t<PL>(const PassArgs&, cudaStream_t); \
+	template cudaError_t launch_row_t<PL>(const PassArgs&, cudaStream_t); \
+	template cudaError_t launch_col_t<PL>(const PassArgs&, cudaStream_t); \
+	template cudaError_t launch_exit_t<PL>(const PassArgs&, cudaStream_t);
 
 } // namespace jms

@@ -47,7 +47,7 @@ def test_unscramble_hash_matches_reference(J):
 
 
 def _oracle_single(J, nx, ny, nobj, ndetper, seed, ntype=1, probe_alpha=22.0, imagedet=G.INT | G.DIF,
-                   islc0=0, nvar=2, dx=0.21, dy=0.17):
+                   islc0=0, nvar=2, dx=0.21, dy=0.17, plans=None):
     """Product vs FP64 oracle on a synthetic specimen of any supported size."""
     from oracle import oracle as OR
 
@@ -68,6 +68,8 @@ def _oracle_single(J, nx, ny, nobj, ndetper, seed, ntype=1, probe_alpha=22.0, im
     for i, (d, m) in enumerate(dets):
         assert J.set_detector(GPU, i, d, m) == 0
     assert J.init_core(GPU) == 0
+    if plans is not None:
+        assert J.L.JMS_SelectPlans(*plans) == 0
     assert J.set_incident_wave(GPU, probe) == 0
     J.seed(seed)
     assert J.offset(GPU, dx, dy, 0.0) == 0
@@ -94,6 +96,33 @@ def test_sizes_match_fp64_oracle(J, nx, ny, nobj, ndetper):
     di, odi, dif, odif = _oracle_single(J, nx, ny, nobj, ndetper, seed=nx + ny)
     assert det_rel(di, odi) < TOL
     assert G.rel_err(dif, odif) < TOL
+
+
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
+def test_every_fft_plan_matches_fp64_oracle(J, n):
+    """Each candidate line plan of a length, on rows and on columns."""
+    import jmultislicelib_b200 as jb
+
+    count = jb.lib().JMS_PlanCount(n)
+    assert count >= 2
+    for i in range(count):
+        di, odi, dif, odif = _oracle_single(J, n, n, 6, 3, seed=n + i, plans=(i, count - 1 - i))
+        assert det_rel(di, odi) < TOL, i
+        assert G.rel_err(dif, odif) < TOL, i
+
+
+def test_autotune_keeps_results(J):
+    import ctypes as C
+
+    di0, odi, _, _ = _oracle_single(J, 512, 512, 8, 4, seed=3)
+    ms_r, ms_c = C.c_float(0), C.c_float(0)
+    ir, ic = C.c_int(-1), C.c_int(-1)
+    assert J.L.JMS_Autotune(4, 3, C.byref(ms_r), C.byref(ms_c), C.byref(ir), C.byref(ic)) == 0
+    assert 0 <= ir.value < J.L.JMS_PlanCount(512) and 0 <= ic.value < J.L.JMS_PlanCount(512)
+    assert ms_r.value > 0 and ms_c.value > 0
+    di1, _, _, _ = _oracle_single(J, 512, 512, 8, 4, seed=3)   # a new setup reuses the tuned plans
+    assert det_rel(di1, odi) < TOL
+    J.L.JMS_SelectPlans(0, 0)
 
 
 def test_planar_propagator_and_start_slice(J):
