@@ -221,6 +221,8 @@ int JmsB200::PropagatorSetup(int whichcode, int npro, const int* proidx)
 	if (npro >= 1 && proidx != nullptr) {
 		npro_ = npro;
 		proidx_.assign(proidx, proidx + nscslc_);
+		pro_k1_.assign(npro, ny_ - 1);
+		pro_k2_.assign(npro, ny_);
 		dfree(d_pro_);
 		const size_t n = (size_t)npro * nx_ * ny_;
 		if ((whichcode & CODE_GPU) && n > 0) {
@@ -320,6 +322,24 @@ int JmsB200::SetPropagatorData(int whichcode, int ipro, const float* pro)
 	if (d_pro_ == nullptr) return 101;
 	if (post(cudaMemcpy(d_pro_ + (size_t)ipro * n, pro, sizeof(float2) * n, cudaMemcpyHostToDevice), "SetPropagatorData"))
 		return 102;
+	// The longest run of all-zero rows (ky) of this propagator: after x P the
+	// wave is exactly zero there, so the passes skip those rows (see PassArgs).
+	int best0 = 0, best1 = -1, run0 = -1;
+	for (int y = 0; y <= ny_; y++) {
+		bool zero = false;
+		if (y < ny_) {
+			zero = true;
+			const float* row = pro + 2 * (size_t)y * nx_;
+			for (int k = 0; k < 2 * nx_ && zero; k++) zero = (row[k] == 0.f);
+		}
+		if (zero && run0 < 0) run0 = y;
+		if (!zero && run0 >= 0) {
+			if (y - 1 - run0 > best1 - best0) { best0 = run0; best1 = y - 1; }
+			run0 = -1;
+		}
+	}
+	if (best1 >= best0) { pro_k1_[ipro] = best0 - 1; pro_k2_[ipro] = best1 + 1; }
+	else { pro_k1_[ipro] = ny_ - 1; pro_k2_[ipro] = ny_; }
 	return 0;
 }
 
@@ -600,20 +620,31 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		if (post(prow_->entry(p, s), "GPUMultislice entry")) return 101;
 		launches_++;
 	}
+	// live Fourier rows (band of the propagator last applied; all after the entry)
+	int in_k1 = ny_ - 1, in_k2 = ny_;
 	for (int j = islc; j < nobjslc_; j++) {
 		const int st = objslc_[j] % nscslc_;
+		const int ip = proidx_[st];
 		PassArgs c = real;
 		c.mul = d_pgr_ + slcoffset_[st] + (long long)var[j] * npgx_ * npgy_;
 		c.npgx = npgx_;
 		c.npgy = npgy_;
 		c.plane = b_img ? plane_of(j) : -1;
+		c.in_k1 = in_k1;
+		c.in_k2 = in_k2;
+		c.out_k1 = pro_k1_[ip];
+		c.out_k2 = pro_k2_[ip];
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
 		if (post(pcol_->col(c, s), "GPUMultislice column pass")) return 401;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
 		PassArgs r = four;
-		r.mul = d_pro_ + (long long)proidx_[st] * N;
+		r.mul = d_pro_ + (long long)ip * N;
 		r.plane = b_dif ? plane_of(j + 1) : -1;
 		r.store = (j + 1 < nobjslc_ || b_img) ? 1 : 0;
+		r.row_k1 = pro_k1_[ip];
+		r.row_k2 = pro_k2_[ip];
+		in_k1 = pro_k1_[ip];
+		in_k2 = pro_k2_[ip];
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
 		if (post(prow_->row(r, s), "GPUMultislice row pass")) return 601;
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
@@ -622,6 +653,8 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 	if (b_img) { // exit plane image readout
 		PassArgs c = real;
 		c.plane = plane_of(nobjslc_);
+		c.in_k1 = in_k1;
+		c.in_k2 = in_k2;
 		if (post(pcol_->exit(c, s), "GPUMultislice exit image")) return 901;
 		launches_++;
 	}

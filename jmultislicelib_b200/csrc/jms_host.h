@@ -163,6 +163,9 @@ private:
 	int status_gpu_ = 0;
 	std::vector<int> nvarslc_, objslc_, det_objslc_, proidx_, detmask_len_, fnx_, fny_;
 	std::vector<long long> slcoffset_;
+	// per propagator: Fourier rows (ky, scrambled index) in (k1, k2) are zero
+	// everywhere (band limit); k1 = ny - 1 when every row has a nonzero value
+	std::vector<int> pro_k1_, pro_k2_;
 	std::vector<float> slcthick_;
 	// rng (CRng: std::mt19937, uniform ints 0..0x7FFFFFFF)
 	std::mt19937 urng_;

@@ -53,6 +53,15 @@ struct PassArgs {
 	int bin_plane = -1;             // plane at which the binned pattern is taken
 	int descan_x = 0, descan_y = 0; // integer-pixel diffraction descan of the Fourier readout
 	int store = 1;                  // row pass: 0 = stop after the readout (last slice)
+	// Band of live Fourier rows: row ky (scrambled index) can be nonzero only
+	// if ky <= k1 or ky >= k2.  Propagators vanish outside their band limit,
+	// so after x P the other rows are exactly zero: the row pass skips them
+	// (row_k1/row_k2, band of its propagator), the column pass reads them as
+	// zero (in_k1/in_k2) and does not store them (out_k1/out_k2, band of the
+	// next row pass).  k1 = ny - 1 marks all rows live.
+	int row_k1 = 1 << 30, row_k2 = 1 << 30;
+	int in_k1 = 1 << 30, in_k2 = 1 << 30;
+	int out_k1 = 1 << 30, out_k2 = 1 << 30;
 	// entry pass source: wav0 (nullptr = the work buffer); with shift set, wav0
 	// is the incident wave and each wave b gets its own probe offset
 	const float2* wav0 = nullptr;   // [ny][nx] Fourier space

@@ -486,14 +486,20 @@ k_row_pass(const PassArgs p)
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
+	// rows outside the propagator's band end up exactly zero: a CTA whose rows
+	// are all outside does nothing, and such rows are neither read nor stored
+	// (the column pass reads them as zero)
+	if (row0 > p.row_k1 && row0 + nval - 1 < p.row_k2) return;
 	float2* W = p.work + (long long)b * p.wstride;
 	float2 v[PL::RM];
 	#pragma unroll
 	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
 	int line, j;
 	T::template role<PL::T>(tid, line, j);
-	if (line < nval) {
-		const float2* src = W + (long long)(row0 + line) * N;
+	const int yl = row0 + line;
+	const bool live = line < nval && (yl <= p.row_k1 || yl >= p.row_k2);
+	if (live) {
+		const float2* src = W + (long long)yl * N;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
@@ -518,9 +524,8 @@ k_row_pass(const PassArgs p)
 	if (READ && p.ndet > 0) block_store_partials<NT>(acc, p, b);
 	if (!p.store) return;
 	PL::template from_mid<true, T>(v, sm, p.twx, tid);
-	T::template role<PL::T>(tid, line, j);
-	if (line < nval) {
-		float2* dst = W + (long long)(row0 + line) * N;
+	if (live) {
+		float2* dst = W + (long long)yl * N;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) dst[j + PL::B * m] = v[m];
 	}
@@ -545,7 +550,10 @@ k_col_pass(const PassArgs p)
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
 		#pragma unroll
-		for (int m = 0; m < PL::A; m++) v[m] = W[(long long)(j + PL::B * m) * nx + c];
+		for (int m = 0; m < PL::A; m++) {
+			const int y = j + PL::B * m;
+			if (y <= p.in_k1 || y >= p.in_k2) v[m] = W[(long long)y * nx + c];
+		}
 	}
 	PL::template to_mid<true, T>(v, sm, p.twy, tid);
 	{
@@ -566,7 +574,10 @@ k_col_pass(const PassArgs p)
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
 		#pragma unroll
-		for (int m = 0; m < PL::A; m++) W[(long long)(j + PL::B * m) * nx + c] = v[m];
+		for (int m = 0; m < PL::A; m++) {
+			const int y = j + PL::B * m;
+			if (y <= p.out_k1 || y >= p.out_k2) W[(long long)y * nx + c] = v[m];
+		}
 	}
 }
 
@@ -589,7 +600,10 @@ k_exit_cols(const PassArgs p)
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
 		#pragma unroll
-		for (int m = 0; m < PL::A; m++) v[m] = W[(long long)(j + PL::B * m) * nx + c];
+		for (int m = 0; m < PL::A; m++) {
+			const int y = j + PL::B * m;
+			if (y <= p.in_k1 || y >= p.in_k2) v[m] = W[(long long)y * nx + c];
+		}
 	}
 	PL::template to_mid<true, T>(v, sm, p.twy, tid);
 	int pos;
