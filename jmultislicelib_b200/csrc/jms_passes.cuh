@@ -561,12 +561,23 @@ k_col_pass(const PassArgs p)
 		T::template role<PL::TMID>(tid, c, pos);
 		if (c < nval && pos < PL::TMID) {
 			const int x = col0 + c;
-			const int xs = x % p.npgx;
-			#pragma unroll
-			for (int e = 0; e < PL::EMID; e++) {
-				const int y = PL::mid(pos, e);
-				if (READ) readout_real(p, b, y, x, v[e]);
-				v[e] = cmul(v[e], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
+			if (p.npgx == nx && p.npgy == p.ny) { // grating of the grid size
+				const float2* t = p.mul + x;
+				#pragma unroll
+				for (int e = 0; e < PL::EMID; e++) {
+					const int y = PL::mid(pos, e);
+					if (READ) readout_real(p, b, y, x, v[e]);
+					v[e] = cmul(v[e], __ldg(t + (long long)y * nx));
+				}
+			}
+			else { // sub-frame grating repeated periodically
+				const int xs = x % p.npgx;
+				#pragma unroll
+				for (int e = 0; e < PL::EMID; e++) {
+					const int y = PL::mid(pos, e);
+					if (READ) readout_real(p, b, y, x, v[e]);
+					v[e] = cmul(v[e], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
+				}
 			}
 		}
 	}
