@@ -247,6 +247,7 @@ def run_ours(args):
     ir, ic = C.c_int(0), C.c_int(0)
     if J.L.JMS_Autotune(min(args.batch, npos_step), 20, C.byref(ms_r), C.byref(ms_c), C.byref(ir), C.byref(ic)):
         raise RuntimeError("autotune failed")
+    print(f"# library kernel launches before the warm-up: {J.L.JMS_KernelLaunches()}", file=sys.stderr)
     names = []
     for axis in (0, 1):
         buf = C.create_string_buffer(64)

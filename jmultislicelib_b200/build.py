@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT}/include"]
 SOURCES = ["jms_kernels.cu", "jms_host.cpp", "jms_generators.cpp", "jms_capi.cpp", "jms_noalloc.cu"] + [
-    f"jms_inst_{k}.cu" for k in range(8)]
+    f"jms_inst_{k}.cu" for k in range(9)]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

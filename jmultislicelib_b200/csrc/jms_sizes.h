@@ -39,6 +39,8 @@ using P768 = Plan<24, 32, 16>;
 using P960 = Plan<30, 32, 16>;
 using P1024a = Plan<32, 32, 16>;
 using P1024b = Plan<32, 32, 8>;
+using P2048a = Plan<32, 64, 8>;
+using P2048b = Plan<32, 64, 4>;
 
 template <class PL> int row_blocks_t(int ny);
 template <class PL> cudaError_t launch_entry_t(const PassArgs& p, cudaStream_t s);
@@ -55,4 +57,5 @@ template <class PL> cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 	X(240, P240, "15x16") X(256, P256a, "16x16 c16") X(256, P256b, "16x16 c8") X(320, P320, "16x20") \
 	X(384, P384, "16x24") X(480, P480, "20x24") X(512, P512a, "16x32 pair c16") X(512, P512b, "8x8x8 c8") \
 	X(512, P512c, "16x32 pair c8") X(640, P640, "20x32") X(720, P720, "24x30") X(768, P768, "24x32") \
-	X(960, P960, "30x32") X(1024, P1024a, "32x32 c16") X(1024, P1024b, "32x32 c8")
+	X(960, P960, "30x32") X(1024, P1024a, "32x32 c16") X(1024, P1024b, "32x32 c8") \
+	X(2048, P2048a, "32x64 pair c8") X(2048, P2048b, "32x64 pair c4")

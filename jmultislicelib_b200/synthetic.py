@@ -162,3 +162,32 @@ def setup_library(J, cfg: dict, specimen: Specimen | None = None):
     else:
         pos = np.array([[0.5 * sp.a, 0.5 * sp.b]], np.float32)
     return sp, probe, pro, dets, pos
+
+
+def random_phase_gratings(nx: int, ny: int, a: float, b: float, ngr: int, seed: int, max_phase: float = 3.0,
+                          smooth: float = 0.03) -> np.ndarray:
+    """Strong-scattering random-phase gratings t = exp(i phi) [ngr, ny, nx].
+
+    phi starts as U(0, 2 pi) per pixel (numpy PCG64, seed), is smoothed by a
+    periodic Gaussian of standard deviation `smooth` nm (0.3 A), and is then
+    rescaled linearly to the range [0, max_phase] rad."""
+    rng = np.random.default_rng(seed)
+    qx = np.fft.fftfreq(nx, d=a / nx)
+    qy = np.fft.fftfreq(ny, d=b / ny)
+    g = np.exp(-2.0 * (np.pi * smooth) ** 2 * (qy[:, None] ** 2 + qx[None, :] ** 2))
+    out = np.empty((ngr, ny, nx), np.complex64)
+    for i in range(ngr):
+        phi = rng.uniform(0.0, 2.0 * np.pi, (ny, nx))
+        phi = np.fft.ifft2(np.fft.fft2(phi) * g).real
+        phi = (phi - phi.min()) * (max_phase / max(phi.max() - phi.min(), 1e-30))
+        out[i] = np.exp(1j * phi)
+    return out
+
+
+# Precision sweep: single probes on strong random-phase gratings (2 slice
+# types alternating, 1 grating each), 200 slices, the pixel size of the
+# 3x3-cell 256^2 grid (11.715 A / 256) on every grid, 300 kV, 25 mrad,
+# aberration free, probe at the cell centre; readout every 10 slices.
+PRECISION_SWEEP = dict(sizes=(256, 512, 1024, 2048), nobj=200, kv=300.0, alpha=25.0, ndetper=10,
+                       dets=((0.0, 10.0), (20.0, 50.0), (80.0, 200.0)), ntype=1, seed=20261205,
+                       pixel=3 * A_CELL / 256, thicknesses=(10, 50, 200))

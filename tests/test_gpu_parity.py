@@ -98,7 +98,7 @@ def test_sizes_match_fp64_oracle(J, nx, ny, nobj, ndetper):
     assert G.rel_err(dif, odif) < TOL
 
 
-@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048])
 def test_every_fft_plan_matches_fp64_oracle(J, n):
     """Each candidate line plan of a length, on rows and on columns."""
     import jmultislicelib_b200 as jb
