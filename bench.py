@@ -326,6 +326,7 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = world * e2e_steps * steps_per_bench_step / e2e_s
+    gen = measure_grating_generation(J, cfg) if rank == 0 else None
 
     if rank == 0:
         N = cfg["nx"] * cfg["ny"]
@@ -353,12 +354,18 @@ def run_ours(args):
                            "batch_waves": args.batch, "parallelism": f"probe positions sharded over {world} GPU(s)",
                            "fft_plans": {"row": names[0], "column": names[1], "tuned_row_us": 1e3 * ms_r.value,
                                          "tuned_col_us": 1e3 * ms_c.value},
-                           "l2": "inputs larger than L2 (128 MiB grating pool, 64 MiB of waves per batch)"},
+                           "l2": f"inputs larger than L2 (128 MiB grating pool, {2 * waves} MiB of waves per "
+                                 "batch, 126 MB L2)"},
                 "e2e": {"value": e2e_value, "unit": UNIT,
                         "h2d_bytes_per_step": int(h_pos.numel() * 4),
                         "d2h_bytes_per_step": int(h_int.numel() * 4 + h_bin.numel() * 4)},
-                "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
+                "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
+                "grating_generation": gen}
         if world == 1 and not args.no_cpu:
+            try:
+                gen["cpu_reference"] = reference_grating_cpu(cfg)
+            except Exception as ex:
+                gen["cpu_reference"] = {"value": None, "sample": f"not run: {ex}"}
             try:
                 nt = host_threads()
                 sample = 8 * nt
@@ -376,6 +383,73 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def measure_grating_generation(J, cfg):
+    """On-device phase gratings (JMS_PgrCalculate) for the workload's specimen:
+    4 slice types x 16 QEP variants of 512^2 gratings (6x6 cells, 72 / 108
+    atoms per slice, Gaussian form factors, sigma 0.08 A displacements,
+    2/3 band limit), written to the generator's own buffer.  Wall-clock time of
+    the host calls (site linking and uploads included), after a warm-up."""
+    import torch
+
+    from jmultislicelib_b200 import synthetic as S
+
+    nx, ny = cfg["nx"], cfg["ny"]
+    a = b = cfg["ncell"] * S.A_CELL
+    ff, sk = S.form_factor_tables(nx, ny, a, b, cfg["seed"], cfg["kv"])
+    if J.pgr_setup(nx, ny, a, b, cfg["kv"], 2, 0, 1) or J.pgr_set_form_factors(ff, sk, [S.BISO_PHONON] * 3):
+        return {"value": None, "unit": "gratings/s", "sample": "generator setup failed"}
+    layers = [S.layer_atoms(cfg["ncell"], cfg["ncell"], st % 2) for st in range(cfg["nslice_types"])]
+
+    def specimen(seed):
+        for st, at in enumerate(layers):
+            e, _ = J.pgr_calculate(at, S.DZ_SLICE, ngr=cfg["nvar"], seed=seed + st, want=False)
+            if e:
+                raise RuntimeError(f"JMS_PgrCalculate returned {e}")
+
+    specimen(1)
+    torch.cuda.synchronize()
+    reps = 5
+    t0 = time.perf_counter()
+    for r in range(reps):
+        specimen(100 * (r + 2))
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / reps
+    ngr = cfg["nslice_types"] * cfg["nvar"]
+    return {"value": ngr / dt, "unit": "gratings/s", "ms_per_specimen": 1e3 * dt,
+            "sample": f"{ngr} gratings of {nx}x{ny} ({cfg['nslice_types']} slice types x {cfg['nvar']} QEP "
+                      f"variants, {len(layers[0])}/{len(layers[1])} atoms per slice) per specimen, {reps} specimens"}
+
+
+def reference_grating_cpu(cfg):
+    """The reference's CJEElaSca::CalculatePhasegratingCPU (one thread, MKL)
+    on slices of the same size and atom count (SrTiO3 6x6 cells: Sr + O and
+    Ti + 2 O layers, Weickenmeier-Kohl form factors)."""
+    from oracle import ref
+
+    from jmultislicelib_b200 import synthetic as S
+
+    if not ref.available():
+        raise RuntimeError("oracle/_ref/libjms_ref.so is not built")
+    n = cfg["ncell"]
+    a = n * S.A_CELL
+    total, count = 0.0, 0
+    for layer in ({(38, 0.0, 0.0), (8, 0.5, 0.5)}, {(22, 0.5, 0.5), (8, 0.5, 0.0), (8, 0.0, 0.5)}):
+        Z, pos = [], []
+        for i in range(n):
+            for j in range(n):
+                for (z, fx, fy) in sorted(layer):
+                    Z.append(z)
+                    pos.append(((i + fx) / n, (j + fy) / n, 0.0))
+        bi = np.full(len(Z), S.BISO_PHONON, np.float32)
+        _, _, _, _, sec = ref.pgr(cfg["nx"], cfg["ny"], a, a, S.DZ_SLICE, cfg["kv"], Z, bi, np.ones(len(Z)), pos,
+                                  thermal=2, nrep=2, seed=5)
+        total += sec
+        count += 2
+    return {"value": count / total, "unit": "gratings/s", "cores": 1, "kind": "reference",
+            "sample": f"{count} gratings of {cfg['nx']}x{cfg['ny']} (72 and 108 atoms), "
+                      f"CJEElaSca::CalculatePhasegratingCPU, {total:.2f} s"}
 
 
 def traffic_from_profiles(kind):

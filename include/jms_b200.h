@@ -191,6 +191,36 @@ int JMS_PlanName(int axis, char* name, int len);
 /* 1 if both grid lengths are supported by the fused passes. */
 int JMS_GridSupported(int nx, int ny);
 
+/* ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273) --------
+ * The 2-D projection mode of CJEElaSca::CalculatePhasegratingGPU
+ * (src/JEElaSca.cpp:978-1159) run on the device: Fourier synthesis of the
+ * projected potential from radial form-factor tables, inverse FFT,
+ * t = exp(i sigma V) (phase reduced in FP64) and the 2/3 band limit.
+ * JMS_PgrSetup: grid nx x ny over the orthorhombic cell a x b [nm]
+ * (SetGrid / CStructure cell), beam energy [keV], thermal model (0 none,
+ * 1 Debye-Waller factors inside the form factors, 2 QEP site displacements),
+ * band limits of the potential (m_bwl_pot, reference default 0) and of the
+ * grating (m_bwl_pgr, default 1).  Returns 0, 1 (bad arguments) or 8
+ * (grid length without a line plan). */
+int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int bwl_pot, int bwl_pgr);
+/* Radial form factors of the atom types: ff [ntype][nk] complex (nm),
+ * sample k at q = k * sk [1/nm] (the table CAtomType::CopyFormFactors returns,
+ * src/Atoms.h:122-125), and Biso [nm^2] per type (QEP amplitudes; may be NULL). */
+int JMS_PgrSetFormFactors(int ntype, int nk, float sk, const float* ff, const float* biso);
+/* ngr phase gratings of one structure slice: atoms [natom][5] = fractional
+ * x, y, z in the cell, occupancy, type index; cz = slice thickness [nm].
+ * Atoms closer than 0.05 nm share a site (CStructure::SetAtomSites,
+ * src/Structure.cpp:441-491); under the QEP model every grating is a new draw
+ * of the site displacements (SplitMix64 stream of seed, Box-Muller).  With
+ * islc >= 0 the gratings become variants ivar0 .. ivar0 + ngr - 1 of
+ * structure slice islc in the multislice setup (PhaseGratingSetup grid must
+ * equal the generator grid); pgr (may be NULL) receives them as complex
+ * [ngr][ny][nx].  Returns 0, 1 (setup incomplete), 2 (bad atom type or
+ * occupancy), 3 (bad arguments), 4 (allocation), 5 (copy), 6/7 (kernels),
+ * 9 (islc / ivar0 / grid do not match the grating setup). */
+int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned long long seed, int islc, int ivar0,
+	float* pgr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,9 @@ SIGNATURES = {
     "JMS_ScanGPUDevice": ([_i, _p, _f, _i, _ip, _p, _p, _i], _i),
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
+    "JMS_PgrSetup": ([_i, _i, _f, _f, _f, _i, _i, _i], _i),
+    "JMS_PgrSetFormFactors": ([_i, _i, _f, _fp, _fp], _i),
+    "JMS_PgrCalculate": ([_i, _fp, _f, _i, C.c_ulonglong, _i, _i, _fp], _i),
     "JMS_ReadoutDetectorsNoAlloc": ([_p, _i, _p, _p], _i),
     "JMS_Autotune": ([_i, _i, _fp, _fp, _ip, _ip], _i),
     "JMS_SelectPlans": ([_i, _i], _i),
@@ -219,6 +222,26 @@ class JMS:
     # additions
     def set_stream(self, stream_ptr):
         return self.L.JMS_SetStream(C.c_void_p(stream_ptr))
+
+    # ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273)
+    def pgr_setup(self, nx, ny, a, b, ekv, thermal=0, bwl_pot=0, bwl_pgr=1):
+        self.pgr_grid = (nx, ny)
+        return self.L.JMS_PgrSetup(nx, ny, a, b, ekv, thermal, bwl_pot, bwl_pgr)
+
+    def pgr_set_form_factors(self, ff, sk, biso=None):
+        ff = _c64(ff)
+        bi = None if biso is None else np.ascontiguousarray(biso, np.float32)
+        return self.L.JMS_PgrSetFormFactors(ff.shape[0], ff.shape[1], sk, _fptr(ff), None if bi is None else _fptr(bi))
+
+    def pgr_calculate(self, atoms, cz, ngr=1, seed=0, islc=-1, ivar0=0, want=True):
+        """atoms [natom, 5]: fractional x, y, z, occupancy, type.  Returns
+        (error, gratings complex64 [ngr, ny, nx] or None)."""
+        at = np.ascontiguousarray(atoms, np.float32).reshape(-1, 5)
+        nx, ny = self.pgr_grid
+        out = np.zeros((ngr, ny, nx), np.complex64) if want else None
+        e = self.L.JMS_PgrCalculate(at.shape[0], _fptr(at), cz, ngr, seed, islc, ivar0,
+                                    None if out is None else _fptr(out))
+        return e, out
 
     def scan(self, pos, npass, dz=0.0, varseq=None, ndetslc=None, ndet=None, bin=0):
         pos = np.ascontiguousarray(pos, np.float32)

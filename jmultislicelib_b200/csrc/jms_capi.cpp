@@ -4,6 +4,7 @@
 #include "../../include/jms_b200.h"
 #include "jms_host.h"
 #include "jms_kernels.h"
+#include "jms_pgr_host.h"
 
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,12 @@ using jms::JmsB200;
 static JmsB200& J()
 {
 	static std::unique_ptr<JmsB200> inst(new JmsB200());
+	return *inst;
+}
+
+static jms::PgrGen& G()
+{
+	static std::unique_ptr<jms::PgrGen> inst(new jms::PgrGen());
 	return *inst;
 }
 
@@ -161,5 +168,27 @@ int JMS_PlanName(int axis, char* name, int len)
 	return 0;
 }
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
+
+int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int bwl_pot, int bwl_pgr)
+{
+	G().Reset();
+	int e = G().SetGrid(nx, ny, a, b);
+	if (e) return e;
+	return G().SetPhysics(ekv, thermal, bwl_pot, bwl_pgr);
+}
+int JMS_PgrSetFormFactors(int ntype, int nk, float sk, const float* ff, const float* biso)
+{ return G().SetFormFactors(ntype, nk, sk, ff, biso); }
+int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned long long seed, int islc, int ivar0,
+	float* pgr)
+{
+	float2* dst = nullptr;
+	if (islc >= 0) {
+		int npgx = 0, npgy = 0;
+		dst = J().GratingSlot(islc, ivar0, ngr, &npgx, &npgy);
+		if (dst == nullptr || npgx != G().nx() || npgy != G().ny()) return 9;
+	}
+	G().SetStream(J().Stream());
+	return G().Calculate(natom, atoms, cz, ngr, seed, dst, pgr);
+}
 
 } // extern "C"

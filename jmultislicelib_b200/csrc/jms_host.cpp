@@ -313,6 +313,15 @@ int JmsB200::SetPhaseGratingData(int whichcode, int islc, int nvar, const float*
 	return 0;
 }
 
+float2* JmsB200::GratingSlot(int islc, int ivar, int nvar, int* npgx, int* npgy)
+{
+	if (d_pgr_ == nullptr || islc < 0 || islc >= nscslc_ || (size_t)islc >= nvarslc_.size()) return nullptr;
+	if (ivar < 0 || nvar < 1 || ivar + nvar > nvarslc_[islc]) return nullptr;
+	if (npgx) *npgx = npgx_;
+	if (npgy) *npgy = npgy_;
+	return d_pgr_ + slcoffset_[islc] + (long long)ivar * npgx_ * npgy_;
+}
+
 int JmsB200::SetPropagatorData(int whichcode, int ipro, const float* pro)
 {
 	if (whichcode & CODE_CPU) return 1;

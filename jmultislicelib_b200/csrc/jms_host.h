@@ -138,6 +138,9 @@ public:
 	int SelectPlans(int irow, int icol);
 	const char* PlanName(int axis) const;
 	int GetScanBatch() const { return scan_batch_; }
+	// device address of grating variants ivar .. ivar + nvar - 1 of structure
+	// slice islc (nullptr if out of the setup), with the grating grid size
+	float2* GratingSlot(int islc, int ivar, int nvar, int* npgx, int* npgy);
 	long long KernelLaunches() const { return launches_; }
 	// Per-pass device timing: with it on, every column / row pass launch is
 	// bracketed by CUDA events on the library stream; PassTiming sums them.

@@ -59,3 +59,12 @@ template <class PL> cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 	X(512, P512c, "16x32 pair c8") X(640, P640, "20x32") X(720, P720, "24x30") X(768, P768, "24x32") \
 	X(960, P960, "30x32") X(1024, P1024a, "32x32 c16") X(1024, P1024b, "32x32 c8") \
 	X(2048, P2048a, "32x64 pair c8") X(2048, P2048b, "32x64 pair c4")
+
+// X(length, plan alias): the default (first) plan of every length in
+// JMS_PLANS, in three groups (used by the phase-grating generator,
+// jms_pgr_ops_*.cu)
+#define JMS_DEFAULT_PLANS_0(X) \
+	X(16, P16) X(24, P24) X(32, P32) X(40, P40) X(48, P48) X(64, P64a) X(80, P80) X(96, P96) X(120, P120) \
+	X(128, P128a) X(160, P160) X(192, P192) X(240, P240) X(256, P256a)
+#define JMS_DEFAULT_PLANS_1(X) X(320, P320) X(384, P384) X(480, P480) X(512, P512a) X(640, P640) X(720, P720)
+#define JMS_DEFAULT_PLANS_2(X) X(768, P768) X(960, P960) X(1024, P1024a) X(2048, P2048a)

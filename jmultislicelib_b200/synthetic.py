@@ -191,3 +191,38 @@ def random_phase_gratings(nx: int, ny: int, a: float, b: float, ngr: int, seed: 
 PRECISION_SWEEP = dict(sizes=(256, 512, 1024, 2048), nobj=200, kv=300.0, alpha=25.0, ndetper=10,
                        dets=((0.0, 10.0), (20.0, 50.0), (80.0, 200.0)), ntype=1, seed=20261205,
                        pixel=3 * A_CELL / 256, thicknesses=(10, 50, 200))
+
+
+# Frozen-phonon displacement of the workloads (sigma 0.08 A per axis) as an
+# isotropic B factor for the on-device grating generator's QEP model:
+# B = 8 pi^2 sigma^2 [nm^2]
+BISO_PHONON = 8.0 * np.pi ** 2 * 0.008 ** 2
+
+
+def layer_atoms(ncell_x: int, ncell_y: int, layer: int) -> np.ndarray:
+    """Atoms of one slice layer for the grating generator: [natom, 5] rows of
+    fractional x, y, z, occupancy, type (0 = A, 1 = B, 2 = O)."""
+    rows = [((ix + fx) / ncell_x, (iy + fy) / ncell_y, 0.0, 1.0, t)
+            for iy in range(ncell_y) for ix in range(ncell_x) for (t, fx, fy) in LAYERS[layer]]
+    return np.asarray(rows, np.float32)
+
+
+def form_factor_tables(nx: int, ny: int, a: float, b: float, seed: int, kv: float = 300.0):
+    """Radial form factors [3, nk] (complex64, nm) of the workload's three
+    Gaussian atom types, sampled as CJEElaSca samples its tables (nk = 12 max(nx,
+    ny), sk = max(nx / a, ny / b) / nk), scaled so that the generator's grating
+    phase c V' (c = lambda / (4 pi a b)) equals sigma V(r):
+        f(q) = (4 pi sigma / lambda) sum_i A_i 2 pi w_i^2 exp(-2 pi^2 w_i^2 q^2).
+    Returns (ff, sk)."""
+    amp, wid = atom_params(seed)
+    nk = 12 * max(nx, ny)
+    sk = max(nx / a, ny / b) / nk
+    e0 = _ME0 * _C0 ** 2 / _QEL / 1000.0
+    lam = _C0 * _HPL / _QEL * 1.0e6 / np.sqrt(kv * (kv + 2 * e0))      # nm
+    k = 4.0 * np.pi * interaction_constant(kv) / lam
+    q = np.arange(nk) * sk
+    ff = np.zeros((3, nk), np.complex64)
+    for t in range(3):
+        ff[t] = k * sum(amp[t, i] * 2 * np.pi * wid[t, i] ** 2 * np.exp(-2 * np.pi ** 2 * wid[t, i] ** 2 * q * q)
+                        for i in range(2))
+    return ff, float(sk)

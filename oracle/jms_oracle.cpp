@@ -19,6 +19,9 @@
  *   - detection plane hash SetDetectionPlanes             src/JMultiSlice.cpp:579-626
  *   - variant draws GetRandomVariantSequence              src/JMultiSlice.cpp:1571-1676
  *     with CRng (std::mt19937 + uniform_int_distribution) src/rng.cpp:30-74
+ *   - phase gratings of CJEElaSca (2-D projection mode)   src/JEElaSca.cpp:486-741, 812-976
+ *     from radial form-factor tables (linear interpolation as
+ *     CAtomType::GetFormFactor, src/Atoms.cpp:414-436)
  *   - unnormalised 2-D C2C transforms as MKL DFTI does    src/JFFTMKLcore.cpp:129-142,176,213
  *     (forward = exp(-i), backward = exp(+i), no scaling), here on a
  *     project-written mixed-radix FP64 FFT.
@@ -337,6 +340,81 @@ int or_multislice(int nx, int ny, double* wav, int nobjslc, int islc0,
 	if (b_img) {
 		fft2d(w, nx, ny, +1);
 		readout_img(nobjslc);
+	}
+	return 0;
+}
+
+// Phase grating of one structure slice, CJEElaSca::CalculatePhasegratingCPU
+// (src/JEElaSca.cpp:812-976) in FP64:
+//   pot(q) = sum_atoms occ ff_type(|q|) ap1(q)^2 exp(-2 pi i (fx fi + fy fj))
+//            (ap1 = 0.5 - 0.5 tanh((|q| / kmax - 0.9) 30) if bwl_pot, else 1;
+//             src/JEElaSca.cpp:590-593, applied in PrepareScatteringFunctions
+//             :733-741 and again in the add :905-913)
+//   V'(r)  = backward transform of pot (unscaled)
+//   t      = exp(i c V'),  c = wl cz / (4 pi vol) with vol = a b cz: the
+//            reference's POT_SCA / vol and PGR_SIG cz wl (:939-950), whose
+//            constant product is 1 / (4 pi)
+//   bwl_pgr: t = backward[ forward[t] * ap2 ], ap2 = 1 / (nx ny) for
+//            |q| <= 2/3 kmax, 0 beyond (:595-602, :956-960).
+// atoms: [natom][2] fractional positions (x / a, y / b) as used (sites,
+// displaced or not); occ [natom]; type [natom]; ff [ntype][nk] complex float.
+int or_pgr(int nx, int ny, double a, double b, double wl, int natom, const double* pos, const float* occ,
+           const int* type, int ntype, int nk, double sk, const float* ff, int bwl_pot, int bwl_pgr, double* out)
+{
+	const long N = (long)nx * ny;
+	zd* t = reinterpret_cast<zd*>(out);
+	const int nx2 = (nx - nx % 2) >> 1, ny2 = (ny - ny % 2) >> 1;
+	const double kmax = std::min(nx2 / a, ny2 / b);
+	std::vector<zd> ex((size_t)natom * nx), ey((size_t)natom * ny);
+	for (int k = 0; k < natom; k++) {
+		if (type[k] < 0 || type[k] >= ntype) return 2;
+		for (int i = 0; i < nx; i++) {
+			double tt = pos[2 * k] * (double)(imod(i + nx2, nx) - nx2);
+			tt -= std::floor(tt);
+			ex[(size_t)k * nx + i] = zd(std::cos(kTwoPi * tt), -std::sin(kTwoPi * tt));
+		}
+		for (int j = 0; j < ny; j++) {
+			double tt = pos[2 * k + 1] * (double)(imod(j + ny2, ny) - ny2);
+			tt -= std::floor(tt);
+			ey[(size_t)k * ny + j] = zd(std::cos(kTwoPi * tt), -std::sin(kTwoPi * tt)) * (double)occ[k];
+		}
+	}
+	auto qabs = [&](int i, int j) {
+		const double qx = (imod(i + nx2, nx) - nx2) / a, qy = (imod(j + ny2, ny) - ny2) / b;
+		return std::sqrt(qx * qx + qy * qy);
+	};
+	parallel_for(ny, [&](int j) {
+		std::vector<zd> fq(ntype);
+		for (int i = 0; i < nx; i++) {
+			const double q = qabs(i, j);
+			double ap = 1.0;
+			if (bwl_pot) ap = 0.5 - 0.5 * std::tanh((q / kmax - 0.9) * 30.0);
+			const double fp = q / sk;
+			int i0 = (int)std::floor(fp);
+			if (i0 > nk - 2) i0 = nk - 2;
+			const double w1 = fp - i0;
+			for (int ty = 0; ty < ntype; ty++) {
+				const float* f = ff + 2 * ((long)ty * nk + i0);
+				fq[ty] = zd(f[0] * (1 - w1) + f[2] * w1, f[1] * (1 - w1) + f[3] * w1) * (ap * ap);
+			}
+			zd acc(0, 0);
+			for (int k = 0; k < natom; k++) acc += fq[type[k]] * ex[(size_t)k * nx + i] * ey[(size_t)k * ny + j];
+			t[(long)j * nx + i] = acc;
+		}
+	});
+	fft2d(t, nx, ny, +1);
+	const double c = wl / (4.0 * std::acos(-1.0) * a * b);
+	for (long i = 0; i < N; i++) {
+		const double ph = c * t[i].real(), am = std::exp(-c * t[i].imag());
+		t[i] = zd(am * std::cos(ph), am * std::sin(ph));
+	}
+	if (bwl_pgr) {
+		fft2d(t, nx, ny, -1);
+		const double kthr = kmax * 2.0 / 3.0;
+		for (int j = 0; j < ny; j++)
+			for (int i = 0; i < nx; i++)
+				t[(long)j * nx + i] *= (qabs(i, j) > kthr) ? 0.0 : 1.0 / (double)N;
+		fft2d(t, nx, ny, +1);
 	}
 	return 0;
 }

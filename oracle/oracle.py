@@ -51,6 +51,8 @@ def lib():
         L.or_multislice.argtypes = [_i, _i, _dp, _i, _i, _fp, _i, _i, _ip, _fp, _ip, _ip,
                                     _i, _fp, _ip, _ip, _i, _d, _dp, _dp, _dp, _dp, _dp]
         L.or_multislice.restype = _i
+        L.or_pgr.argtypes = [_i, _i, _d, _d, _d, _i, _dp, _fp, _ip, _i, _i, _d, _fp, _i, _i, _dp]
+        L.or_pgr.restype = _i
         _lib = L
     return _lib
 
@@ -159,3 +161,21 @@ def multislice(wav, pgr_pool, pgr_idx, pro_pool, pro_idx, det_objslc, ndetslc, d
     assert e == 0
     acc["wave"] = w
     return acc
+
+
+def pgr(nx, ny, a, b, wl, pos, occ, atype, ff, sk, bwl_pot=0, bwl_pgr=1) -> np.ndarray:
+    """Phase grating of CJEElaSca::CalculatePhasegratingCPU (src/JEElaSca.cpp:812-976)
+    in FP64.  pos [natom, 2] fractional (x/a, y/b) of the atoms as placed;
+    occ, atype per atom; ff complex [ntype, nk] radial form factors sampled
+    every sk 1/nm.  Returns complex128 [ny, nx]."""
+    natom = len(occ)
+    p = np.ascontiguousarray(pos, np.float64).reshape(natom, 2)
+    o, po = _f32(occ)
+    t, pt = _i32(atype)
+    f, pf = _f32(np.asarray(ff, np.complex64))
+    ntype, nk = f.shape
+    out = np.zeros((ny, nx), np.complex128)
+    e = lib().or_pgr(nx, ny, a, b, wl, natom, p.ctypes.data_as(_dp), po, pt, ntype, nk, sk, pf, bwl_pot, bwl_pgr,
+                     out.ctypes.data_as(_dp))
+    assert e == 0, e
+    return out

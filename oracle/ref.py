@@ -85,6 +85,8 @@ def lib():
             "ref_calc_propagator": ([_p, _f, _f, _f, _i, _fp], _i),
             "ref_calc_ring_detector": ([_p, _f, _f, _f, _f, _f, _f, C.c_char_p, _fp, _ip, _ip, _i], _i),
             "ref_cpu_scan": ([C.POINTER(_p), _i, _i, _fp, _i, _i, _fp], _i),
+            "ref_pgr": ([_i, _i, _f, _f, _f, _f, _i, _i, _f, _i, _ip, _fp, _fp, _fp, _i, _i, _fp, _ip, _fp, _ip, _fp,
+                         _ip, C.POINTER(C.c_double)], _i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -263,3 +265,36 @@ def cpu_scan(objs, npos_xy: np.ndarray, nrepeat: int, ndetout: int) -> tuple[np.
     finally:
         torch.set_num_threads(nt0)
     return out, e
+
+
+def pgr(nx, ny, a, b, c, ekv, Z, biso, occ, pos, thermal=0, absorb=0, abf=0.0, nrep=1, seed=0):
+    """Phase grating(s) of one structure slice by the reference's CJEElaSca CPU
+    path (src/JEElaSca.cpp:812-976): Z, biso [nm^2], occ per atom, pos [natom, 3]
+    fractional.  Returns (pgr complex64 [nrep, ny, nx], atom_type [natom],
+    ff complex64 [ntype, nk], sk, seconds)."""
+    import torch  # noqa: F401  (MKL lives in libtorch_cpu)
+
+    L = lib()
+    natom = len(Z)
+    Z = np.ascontiguousarray(Z, np.int32)
+    biso = np.ascontiguousarray(biso, np.float32)
+    occ = np.ascontiguousarray(occ, np.float32)
+    pos = np.ascontiguousarray(pos, np.float32).reshape(natom, 3)
+    out = np.zeros((nrep, ny, nx), np.complex64)
+    at = np.zeros(natom, np.int32)
+    cap = 12 * max(nx, ny)
+    ff = np.zeros((natom, cap), np.complex64)
+    nk = C.c_int(cap)
+    sk = C.c_float(0)
+    nt = C.c_int(0)
+    sec = C.c_double(0)
+    nt0 = torch.get_num_threads()
+    torch.set_num_threads(1)
+    try:
+        e = L.ref_pgr(nx, ny, a, b, c, ekv, thermal, absorb, abf, natom, iptr(Z), fptr(biso), fptr(occ), fptr(pos),
+                      nrep, seed, fptr(out), iptr(at), fptr(ff), C.byref(nk), C.byref(sk), C.byref(nt),
+                      C.byref(sec))
+    finally:
+        torch.set_num_threads(nt0)
+    assert e == 0, e
+    return out, at, ff[:nt.value, :nk.value].copy(), sk.value, sec.value

@@ -9,10 +9,14 @@
  * the product links or loads this file.
  *
  * Every function forwards to the reference method of the same name; no
- * reference source is copied here.
+ * reference source is copied here.  ref_pgr drives the reference's phase
+ * grating calculation (CJEElaSca, src/JEElaSca.h:98-273) on its CPU path.
  */
 #include "JMultiSlice.h"
+#include "JEElaSca.h"
+#include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <dlfcn.h>
 #include <thread>
 #include <vector>
@@ -26,6 +30,12 @@ public:
 	fcmplx* cpu_wave(int ithread) { // thread wave slot after OffsetIncomingWave (JMultiSlice.cpp:2024)
 		return m_h_wav + (int64_t)m_nscx * m_nscy * ithread;
 	}
+};
+
+// Exposes the prepared atom types (radial form factors) of CJEElaSca.
+class RefEElaSca : public CJEElaSca {
+public:
+	const std::vector<CAtomType>& types() const { return m_vTypes; }
 };
 
 extern "C" {
@@ -141,6 +151,68 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	}
 	for (auto& th : pool) th.join();
 	return err.load();
+}
+
+// Phase grating(s) of one structure slice by the reference's CJEElaSca on the
+// CPU path: CStructure::AddAtom per atom (Z, Biso [nm^2], occupancy,
+// fractional x, y, z), SetAtomSites(0.05), cell (a, b, c) [nm] at 90 degrees
+// with the identity basis; SetGrid(nx, ny, 1, 0), SetPhysics(ekv, 0, absorb,
+// abf, thermal), CalculateFormFactors, PrepareScatteringFunctions(-1, 1),
+// then nrep x CalculatePhasegratingCPU (thread 0) after SeedRngEx(seed).
+// Outputs: pgr [nrep][ny][nx] complex, atom_type [natom] (type index of each
+// atom), ff [ntype][nk] complex and sk of the prepared types (ff may be NULL;
+// *nk_io in: capacity per type, out: nk), *ntype_out, *seconds (time of the
+// nrep grating calls).  Returns 0 or the first reference error + 100 * stage.
+int ref_pgr(int nx, int ny, float a, float b, float c, float ekv, int thermal, int absorb, float abf, int natom,
+	const int* Z, const float* biso, const float* occ, const float* pos, int nrep, int seed, float* pgr,
+	int* atom_type, float* ff, int* nk_io, float* sk_out, int* ntype_out, double* seconds)
+{
+	CStructure st;
+	st.m_vCellSize = CV3D(a, b, c);
+	st.m_vCellAngles = CV3D(90.f, 90.f, 90.f);
+	for (int i = 0; i < natom; i++)
+		st.AddAtom(Z[i], 0.f, biso[i], occ[i], pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+	st.SetAtomSites(0.05f);
+	RefEElaSca E;
+	int e;
+	if ((e = E.SetStructure(st))) return 100 + e;
+	if ((e = E.SetGrid((unsigned)nx, (unsigned)ny, 1u, 0u))) return 200 + e;
+	if ((e = E.SetPhysics(ekv, 0u, (unsigned)absorb, abf, (unsigned)thermal))) return 300 + e;
+	if ((e = E.CalculateFormFactors(false))) return 400 + e;
+	if ((e = E.PrepareScatteringFunctions(-1, 1, false))) return 500 + e;
+	E.SeedRngEx(seed);
+	const size_t N = (size_t)nx * ny;
+	auto t0 = std::chrono::steady_clock::now();
+	for (int r = 0; r < nrep; r++) {
+		if ((e = E.CalculatePhasegratingCPU(&st, (fcmplx*)(pgr + 2 * N * r), 0))) return 600 + e;
+	}
+	auto t1 = std::chrono::steady_clock::now();
+	if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+	for (int i = 0; i < natom; i++) atom_type[i] = st.m_vAtoms[i].m_nAtomTypeIndex;
+	// the prepared radial tables: CAtomType::CopyFormFactors (src/Atoms.cpp:106-127)
+	// never hands its buffer back, so the samples are read with GetFormFactor
+	// at q = k sk (linear interpolation there returns the sample); nk and sk
+	// as CalculateFormFactors sets them (src/JEElaSca.cpp:459-462)
+	const auto& ty = E.types();
+	if (ntype_out) *ntype_out = (int)ty.size();
+	const int nk = 12 * std::max(std::max(nx, ny), 1);
+	const float sk = std::max(std::max((float)nx / a, (float)ny / b), 1.f / c) / (float)nk;
+	if (nk_io) {
+		const int cap = *nk_io;
+		*nk_io = nk;
+		if (ff && nk <= cap) {
+			for (size_t t = 0; t < ty.size(); t++) {
+				CAtomType& T = const_cast<CAtomType&>(ty[t]);
+				for (int k = 0; k < nk; k++) {
+					const fcmplx v = T.GetFormFactor(sk * (float)std::min(k, nk - 2), 1);
+					ff[2 * ((size_t)cap * t + k)] = v.real();
+					ff[2 * ((size_t)cap * t + k) + 1] = v.imag();
+				}
+			}
+		}
+	}
+	if (sk_out) *sk_out = sk;
+	return 0;
 }
 
 } // extern "C"
