@@ -191,6 +191,18 @@ int JMS_PlanName(int axis, char* name, int len);
 /* 1 if both grid lengths are supported by the fused passes. */
 int JMS_GridSupported(int nx, int ny);
 
+/* Detector readouts of the averaged wave functions: the public method
+ * CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.h:935, .cpp:2667-2945), GPU
+ * branch, which the reference's flat interface does not export.  whichresult
+ * JMS_DETECT_INTEGRATED: dst[idetslc * ndet + idet] = sum_k |<psi(k)>|^2 D(k)
+ * over the averaged Fourier-space waves (WAVEF_AVG); JMS_DETECT_IMAGE /
+ * JMS_DETECT_DIFFRACTION: dst [ndetslc][ny][nx] = |<psi(r)>|^2 / |<psi(k)>|^2
+ * of the averaged real-space / Fourier-space waves.  Each needs its detection
+ * flag and the averaged wave; *weight = the wave averaging weight (the sums
+ * are not divided by it).  Returns 0 (also when there is nothing to read),
+ * 1 for the CPU code, or 21-23 / 121-122 on device errors. */
+int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight);
+
 /* ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273) --------
  * The 2-D projection mode of CJEElaSca::CalculatePhasegratingGPU
  * (src/JEElaSca.cpp:978-1159) run on the device: Fourier synthesis of the

@@ -69,6 +69,7 @@ SIGNATURES = {
     "JMS_ScanGPUDevice": ([_i, _p, _f, _i, _ip, _p, _p, _i], _i),
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
+    "JMS_ReadoutDetAvg": ([_i, _i, _fp, _fp], _i),
     "JMS_PgrSetup": ([_i, _i, _f, _f, _f, _i, _i, _i], _i),
     "JMS_PgrSetFormFactors": ([_i, _i, _f, _fp, _fp], _i),
     "JMS_PgrCalculate": ([_i, _fp, _f, _i, C.c_ulonglong, _i, _i, _fp], _i),
@@ -210,6 +211,13 @@ class JMS:
         w = C.c_float(0)
         self.L.GetAvgResult(code, which, dst.view(np.float32).ctypes.data_as(_fp), C.byref(w), 0)
         return dst, w.value
+
+    def readout_det_avg(self, which, count):
+        """CJMultiSlice::ReadoutDetAvg on the device: (error, dst, weight)."""
+        dst = np.zeros(count, np.float32)
+        w = C.c_float(0)
+        e = self.L.JMS_ReadoutDetAvg(CODE_GPU, which, _fptr(dst), C.byref(w))
+        return e, dst, w.value
 
     def unscramble_hash(self):
         out = np.zeros(self.nx * self.ny, np.uint32)

@@ -169,6 +169,9 @@ int JMS_PlanName(int axis, char* name, int len)
 }
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
 
+int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight)
+{ return J().ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }
+
 int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int bwl_pot, int bwl_pgr)
 {
 	G().Reset();

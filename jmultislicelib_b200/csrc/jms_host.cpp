@@ -756,6 +756,62 @@ int JmsB200::GetAvgResult(int whichcode, int whichresult, float* dst, float* wei
 	return 0;
 }
 
+int JmsB200::ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight, int)
+{
+	// Readouts of the averaged wave functions (elastic channel): integrated
+	// detectors on |<psi(k)>|^2, or the pattern |<psi>|^2 per plane.  Gating
+	// as in the reference: the detection flag of the requested result must be
+	// set and the averaged wave it is read from must exist.
+	if (weight) *weight = 0.f;
+	if (whichcode & CODE_CPU) return 1;
+	if (!(whichcode & CODE_GPU) || dst == nullptr) return 0;
+	if (weight) *weight = weight_wavavg_;
+	if (!(d_wfr_avg_ || d_wff_avg_) || ndetslc_ <= 0) return 0;
+	cudaStream_t s = stream_;
+	const long long N = (long long)nx_ * ny_;
+	switch (whichresult) {
+	case DET_INTEGRATED: {
+		if (ndet_ <= 0 || !(imagedet_ & DET_INTEGRATED) || d_wff_avg_ == nullptr || d_det_ == nullptr) return 0;
+		double* d_out = nullptr;
+		if (post(cudaMalloc(&d_out, sizeof(double) * ndetslc_ * ndet_), "ReadoutDetAvg")) return 21;
+		int e = launch_readout_noalloc(d_wff_avg_, ndetslc_, nx_, ny_, d_det_, ndet_, d_out, s);
+		if (e == 0) launches_ += 2;
+		if (e == 131) {   // too many partial sums at once: one plane at a time
+			e = 0;
+			for (int p = 0; p < ndetslc_ && e == 0; p++) {
+				e = launch_readout_noalloc(d_wff_avg_ + p * N, 1, nx_, ny_, d_det_, ndet_, d_out + (long long)p * ndet_, s);
+				if (e == 0) launches_ += 2;
+			}
+		}
+		std::vector<double> h((size_t)ndetslc_ * ndet_);
+		if (e == 0 && post(cudaMemcpyAsync(h.data(), d_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s),
+			"ReadoutDetAvg")) e = 22;
+		if (e == 0 && post(cudaStreamSynchronize(s), "ReadoutDetAvg")) e = 22;
+		cudaFree(d_out);
+		if (e) return e == 22 ? 22 : 23;
+		for (size_t i = 0; i < h.size(); i++) dst[i] = (float)h[i];   // [idetslc][idet]
+		return 0;
+	}
+	case DET_IMAGE:
+	case DET_DIFFRACTION: {
+		const float2* src = (whichresult == DET_IMAGE) ? d_wfr_avg_ : d_wff_avg_;
+		if (!(imagedet_ & whichresult) || src == nullptr) return 0;
+		float* d_out = nullptr;
+		const long long n = N * ndetslc_;
+		if (post(cudaMalloc(&d_out, sizeof(float) * n), "ReadoutDetAvg")) return 121;
+		int e = post(launch_abs2(d_out, src, n, s), "ReadoutDetAvg") ? 121 : 0;
+		if (!e) launches_ += 1;
+		if (!e && post(cudaMemcpyAsync(dst, d_out, sizeof(float) * n, cudaMemcpyDeviceToHost, s), "ReadoutDetAvg"))
+			e = 122;
+		if (!e && post(cudaStreamSynchronize(s), "ReadoutDetAvg")) e = 122;
+		cudaFree(d_out);
+		return e;
+	}
+	default:
+		return 0;
+	}
+}
+
 float JmsB200::GetImageAveragingWeight(int whichcode, int) const { return (whichcode & CODE_GPU) ? weight_imgavg_ : 0.f; }
 float JmsB200::GetWaveAveragingWeight(int whichcode, int) const { return (whichcode & CODE_GPU) ? weight_wavavg_ : 0.f; }
 

@@ -102,6 +102,9 @@ public:
 	int GPUMultislice(int islc0, int accmode, float weight);
 	int GetResult(int whichcode, int whichresult, float* dst, int iThread);
 	int GetAvgResult(int whichcode, int whichresult, float* dst, float* weight, int iThread);
+	// CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.cpp:2667-2945), GPU branch:
+	// detector readouts of the averaged waves
+	int ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight, int iThread);
 	float GetImageAveragingWeight(int whichcode, int iThread) const;
 	float GetWaveAveragingWeight(int whichcode, int iThread) const;
 	int ResetImageAveraging(int whichcode, int iThread);

@@ -29,6 +29,14 @@ __global__ void k_make_shift(double* sh, const float* __restrict__ pos, int npos
 	sh[4 * i + 3] = fz / (b * b);
 }
 
+__global__ void k_abs2(float* __restrict__ out, const float2* __restrict__ in, long long n)
+{
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const float2 v = in[i];
+	out[i] = v.x * v.x + v.y * v.y;
+}
+
 __global__ void k_finalize(const float* __restrict__ partial, int n, int nblk, float weight, double* det_int)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -91,6 +99,13 @@ cudaError_t launch_make_shift(double* d_shift, const float* d_pos, int npos, dou
 	cudaStream_t s)
 {
 	k_make_shift<<<(npos + 127) / 128, 128, 0, s>>>(d_shift, d_pos, npos, a, b, fz);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_abs2(float* out, const float2* in, long long n, cudaStream_t s)
+{
+	if (n <= 0) return cudaSuccess;
+	k_abs2<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, in, n);
 	return cudaGetLastError();
 }
 

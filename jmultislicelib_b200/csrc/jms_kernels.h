@@ -103,6 +103,9 @@ int launch_readout_noalloc(const float2* wav, int nwave, int nx, int ny, const f
 	cudaStream_t s);
 int noalloc_capacity();
 
+// out[i] = |in[i]|^2, i < n
+cudaError_t launch_abs2(float* out, const float2* in, long long n, cudaStream_t s);
+
 // drop-in OffsetIncomingWave: out = wav0(k - tilt) * exp(-i(2 pi turns + cppl))
 cudaError_t launch_offset(float2* out, const float2* wav0, int nx, int ny, const double* shift_host4,
 	const float* cppl, int ibtx, int ibty, cudaStream_t s);

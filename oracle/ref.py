@@ -85,6 +85,7 @@ def lib():
             "ref_calc_propagator": ([_p, _f, _f, _f, _i, _fp], _i),
             "ref_calc_ring_detector": ([_p, _f, _f, _f, _f, _f, _f, C.c_char_p, _fp, _ip, _ip, _i], _i),
             "ref_cpu_scan": ([C.POINTER(_p), _i, _i, _fp, _i, _i, _fp], _i),
+            "ref_readout_det_avg": ([_p, _i, _i, _fp, _fp, _i], _i),
             "ref_pgr": ([_i, _i, _f, _f, _f, _f, _i, _i, _f, _i, _ip, _fp, _fp, _fp, _i, _i, _fp, _ip, _fp, _ip, _fp,
                          _ip, C.POINTER(C.c_double)], _i),
         }
@@ -226,6 +227,13 @@ class RefJMS:
         w = C.c_float(0)
         self.L.ref_get_avg_result(self.h, code, which, dst.view(np.float32).ctypes.data_as(_fp), C.byref(w), ithread)
         return dst, w.value
+
+    def readout_det_avg(self, code, which, count, ithread=0):
+        """CJMultiSlice::ReadoutDetAvg: (error, dst, weight)."""
+        dst = np.zeros(count, np.float32)
+        w = C.c_float(0)
+        e = lib().ref_readout_det_avg(self.h, code, which, fptr(dst), C.byref(w), ithread)
+        return e, dst, w.value
 
     def cpu_wave(self, ithread=0):
         out = np.zeros((self.ny, self.nx), np.complex64)

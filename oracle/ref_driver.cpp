@@ -153,6 +153,15 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	return err.load();
 }
 
+// CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.cpp:2667-2945).
+int ref_readout_det_avg(void* h, int whichcode, int whichresult, float* dst, float* weight, int ithread)
+{
+	float w = 0.f;
+	int e = ((RefJMS*)h)->ReadoutDetAvg(whichcode, whichresult, dst, w, ithread);
+	if (weight) *weight = w;
+	return e;
+}
+
 // Phase grating(s) of one structure slice by the reference's CJEElaSca on the
 // CPU path: CStructure::AddAtom per atom (Z, Biso [nm^2], occupancy,
 // fractional x, y, z), SetAtomSites(0.05), cell (a, b, c) [nm] at 90 degrees

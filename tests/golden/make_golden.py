@@ -170,6 +170,13 @@ def make_case(g, name, nx, ny, a, b, kv, nvar, objslc, thick, proidx, protype, t
             g[p + key + "_w"] = np.float32(wgt)
     if name == "msa":
         g[p + "unscramble"] = R.unscramble_hash()
+    if imagedet & (WFR_AVG | WFF_AVG):   # CJMultiSlice::ReadoutDetAvg of the averaged waves
+        for flag, key, cnt in ((INT, "rda_int", nd * len(dets)), (IMG, "rda_img", nd * N), (DIF, "rda_dif", nd * N)):
+            if imagedet & flag:
+                e, arr, wgt = R.readout_det_avg(CPU, flag, cnt)
+                assert e == 0, e
+                g[p + key] = arr
+                g[p + "rda_w"] = np.float32(wgt)
     R.close()
 
 
@@ -193,6 +200,10 @@ def multislice_cases(g):
     make_case(g, "msd", 32, 32, 0.9, 0.9, 300.0, [3], [0] * 8, [0.2], [0], 1, (0.0, 0.0), ring[:2], 4,
               INT | IMG_AVG | DIF_AVG | WFR_AVG | WFF_AVG,
               [(0.1, 0.1, 0.0, 0, 0, 0, 1 / 3), (0.2, 0.3, 0.0, 0, 0, 0, 1 / 3), (0.4, 0.0, 0.0, 0, 0, 0, 1 / 3)], 17)
+    # G: readouts of the averaged waves (ReadoutDetAvg) over three weighted runs.
+    make_case(g, "msg", 48, 48, 1.0, 1.0, 300.0, [3, 2], [0, 1] * 5, [0.19525], [0, 0], 1, (0.0, 0.0), ring[:3],
+              5, INT | IMG | DIF | WFR_AVG | WFF_AVG,
+              [(0.1, 0.2, 0.0, 0, 0, 0, 0.5), (0.3, 0.1, 0.0, 0, 0, 1, 0.25), (0.2, 0.4, 0.0, 0, 0, 1, 0.25)], 29)
     # E: start slice > 0, probe beam tilt in pixels and a constant phase plate.
     make_case(g, "mse", 64, 64, 1.2, 1.2, 300.0, [2, 2], [0, 1] * 5, [0.19525], [0, 0], 1, (0.0, 0.0), ring[:3],
               3, INT | DIF | IMG, [(0.2, 0.1, 0.5, 2, -1, 0, 1.0)], 21, islc0=4, cppl_seed=3)

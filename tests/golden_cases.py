@@ -17,7 +17,7 @@ _cache = None
 
 INT, IMG, DIF, WFR, WFF = 1, 2, 4, 8, 16
 IMG_AVG, DIF_AVG, WFR_AVG, WFF_AVG = 32, 64, 128, 256
-CASES = ("msa", "msb", "msc", "msd", "mse", "msf")
+CASES = ("msa", "msb", "msc", "msd", "mse", "msf", "msg")
 
 
 def golden():

@@ -57,6 +57,14 @@ def run_case(J, name):
             arr, w = J.get_avg_result(GPU, flag, nd * N, dt)
             out[key] = arr.reshape(shp)
             out[key + "_w"] = w
+    if im & (G.WFR_AVG | G.WFF_AVG):   # ReadoutDetAvg of the averaged waves
+        for flag, key, cnt in ((G.INT, "rda_int", nd * c["ndet"]), (G.IMG, "rda_img", nd * N),
+                               (G.DIF, "rda_dif", nd * N)):
+            if im & flag:
+                e, arr, w = J.readout_det_avg(flag, cnt)
+                assert e == 0, e
+                out[key] = arr
+                out["rda_w"] = w
     return c, out
 
 

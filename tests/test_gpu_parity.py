@@ -39,6 +39,13 @@ def test_golden_case_matches_reference(J, name):
     for key in ("img_avg", "dif_avg", "wfr_avg", "wff_avg"):
         if key in c:
             assert abs(out[key + "_w"] - float(c[key + "_w"])) < 1e-6
+    if "rda_int" in c:   # CJMultiSlice::ReadoutDetAvg
+        nd = int(c["ndetslc"])
+        assert det_rel(out["rda_int"].reshape(nd, -1), c["rda_int"].reshape(nd, -1)) < TOL
+        assert abs(out["rda_w"] - float(c["rda_w"])) < 1e-6
+    for key in ("rda_img", "rda_dif"):
+        if key in c:
+            assert G.rel_err(out[key], c[key]) < TOL, key
 
 
 def test_unscramble_hash_matches_reference(J):

@@ -92,3 +92,35 @@ def test_norm_conservation():
     res = OR.multislice(wav, pgr.astype(np.complex64), np.arange(6) % 2, pro.astype(np.complex64)[None],
                         np.zeros(6, np.int32), hsh, 7, det=det, imagedet=1)
     np.testing.assert_allclose(res["det_int"][:, 0], 1.0, rtol=1e-6)
+
+
+def _det_eff(c):
+    """Detector functions with their masks folded in (a masked detector counts
+    only its listed pixels; an unmasked one the whole grid)."""
+    out = []
+    for d, m in zip(c["det"], c["msk"]):
+        d = np.asarray(d, np.float64).ravel()
+        if len(m):
+            e = np.zeros_like(d)
+            e[np.asarray(m)] = d[np.asarray(m)]
+            d = e
+        out.append(d)
+    return np.stack(out)
+
+
+@pytest.mark.parametrize("name", ["msd", "msg"])
+def test_readout_det_avg_matches_reference(name):
+    """CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.cpp:2667-2945) on the
+    oracle's averaged waves: integrated detectors on |<psi(k)>|^2 and the
+    |<psi>|^2 patterns."""
+    c = G.case(name)
+    o = G.oracle_case(name)
+    nd = int(c["ndetslc"])
+    wff = o["avg"]["wff"].reshape(nd, -1)
+    want = (np.abs(wff) ** 2) @ _det_eff(c).T
+    assert G.rel_err(c["rda_int"].reshape(nd, -1), want) < 2e-5
+    assert abs(float(c["rda_w"]) - o["avg"]["w"]) < 1e-6
+    if "rda_img" in c:
+        assert G.rel_err(c["rda_img"].reshape(o["avg"]["wfr"].shape), np.abs(o["avg"]["wfr"]) ** 2) < 2e-5
+    if "rda_dif" in c:
+        assert G.rel_err(c["rda_dif"].reshape(o["avg"]["wff"].shape), np.abs(o["avg"]["wff"]) ** 2) < 2e-5
