@@ -77,7 +77,10 @@ void SetSupercellSize(float* a0);                /* src/JMultiSliceLib.h:138 */
 void SetSupercellSizeABC(float a, float b, float c); /* src/JMultiSliceLib.h:141 */
 void SetSliceThickness(int islc, float fthickness);  /* src/JMultiSliceLib.h:146 */
 void DiffractionDescan(int bActivate);           /* src/JMultiSliceLib.h:149 (bool) */
-void SetPlasmonMC(int bActivate, float fq_e, float fq_c, float fmfp, unsigned int nexmax); /* :152; activating it makes GPUMultislice return 5 */
+void SetPlasmonMC(int bActivate, float fq_e, float fq_c, float fmfp, unsigned int nexmax); /* :152; bulk plasmon
+	Monte-Carlo: q_e, q_c [1/nm], mean free path [nm], max. excitations; the pixel shift of each slice is drawn
+	on the host from the library RNG after the variant draw (CJPlasmonMC::ScatGridMC) and applied in the
+	column pass */
 void SetDiffractionDescanN(int whichcode, int ndescanx, int ndescany, int iThread);       /* :160 */
 void SetDiffractionDescan(int whichcode, float descanx, float descany, int iThread);     /* :168 */
 void SetDiffractionDescanMRad(int whichcode, float descanx, float descany, int iThread); /* :176 */

@@ -40,7 +40,8 @@ void SetSupercellSize(float* a0) { if (a0) J().SetSupercellSize(a0[0], a0[1], a0
 void SetSupercellSizeABC(float a, float b, float c) { J().SetSupercellSize(a, b, c); }
 void SetSliceThickness(int islc, float fthickness) { J().SetSliceThickness(islc, fthickness); }
 void DiffractionDescan(int bActivate) { J().DiffractionDescan(bActivate != 0); }
-void SetPlasmonMC(int bActivate, float, float, float, unsigned int nexmax) { J().SetPlasmonMC(bActivate != 0, nexmax); }
+void SetPlasmonMC(int bActivate, float fq_e, float fq_c, float fmfp, unsigned int nexmax)
+{ J().SetPlasmonMC(bActivate != 0, fq_e, fq_c, fmfp, nexmax); }
 void SetDiffractionDescanN(int whichcode, int ndescanx, int ndescany, int) { J().SetDiffractionDescanN(whichcode, ndescanx, ndescany); }
 void SetDiffractionDescan(int whichcode, float descanx, float descany, int) { J().SetDiffractionDescan(whichcode, descanx, descany); }
 void SetDiffractionDescanMRad(int whichcode, float descanx, float descany, int) { J().SetDiffractionDescanMRad(whichcode, descanx, descany); }

@@ -126,6 +126,45 @@ double JmsB200::unirand(double a, double b)
 	return a + ((double)uni_(urng_) / (double)((unsigned long)0x7FFFFFFF)) * (b - a);
 }
 
+void JmsB200::SetPlasmonMC(bool use, float q_e, float q_c, float mfp, unsigned int nexmax)
+{
+	plasmon_on_ = (use && nexmax > 0) ? 1 : 0;
+	pl_qe_ = std::fabs(q_e);
+	pl_qc_ = std::fabs(q_c);
+	pl_mfp_ = std::fabs(mfp);
+	pl_nmax_ = nexmax;
+}
+
+int JmsB200::plasmon_step(float dt, int* di, int* dj)
+{
+	// CJPlasmonMC::ScatteringMC / ScatGridMC (src/JPlasmonMC.cpp:168-209) on
+	// the library RNG: a Poisson number of new excitations (mean dt / mfp,
+	// capped at the remaining excitation budget), each scattering by q with
+	// q^2 = qe^2 ((qc/qe)^2 + 1)^u - qe^2 (u uniform) in a uniform direction;
+	// the wave moves by the change of round(q_total * a) pixels
+	*di = *dj = 0;
+	if (pl_mfp_ <= 0.f || pl_qe_ <= 0.f || pl_qc_ < pl_qe_) return 0;
+	std::poisson_distribution<int> pd((double)(dt / pl_mfp_));
+	const unsigned int n = std::min((unsigned int)pd(urng_), pl_nmax_ - pl_nex_);
+	if (n == 0) return 0;
+	const float qe2 = pl_qe_ * pl_qe_, qc2 = pl_qc_ * pl_qc_;
+	float qx = 0.f, qy = 0.f;
+	for (unsigned int i = 0; i < n; i++) {
+		const float phi = (float)(6.283185307179586 * unirand(0.0, 1.0));
+		const float u = (float)unirand(0.0, 1.0);
+		const float q = std::sqrt(qe2 * std::pow(qc2 / qe2 + 1.f, u) - qe2);
+		qx += q * std::cos(phi);
+		qy += q * std::sin(phi);
+	}
+	const int i0 = (int)std::round(pl_tqx_ * a0_[0]), j0 = (int)std::round(pl_tqy_ * a0_[1]);
+	pl_nex_ += n;
+	pl_tqx_ += qx;
+	pl_tqy_ += qy;
+	*di = (int)std::round(pl_tqx_ * a0_[0]) - i0;
+	*dj = (int)std::round(pl_tqy_ * a0_[1]) - j0;
+	return (int)n;
+}
+
 int JmsB200::GetRandomVariantSequence(int* out)
 {
 	if (!out) return 1;
@@ -576,7 +615,7 @@ int JmsB200::ensure_partial(int nwave)
 // of GPUMultislice (src/JMultiSlice.cpp:4611-4666).
 int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src,
 	const double* d_shift, int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx,
-	int nby)
+	int nby, const int* plas, const int* d_plas_w)
 {
 	if (!prow_ || !pcol_) return 2;
 	if (ensure_work(nwave) || ensure_partial(nwave)) return 1;
@@ -643,6 +682,8 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		c.in_k2 = in_k2;
 		c.out_k1 = pro_k1_[ip];
 		c.out_k2 = pro_k2_[ip];
+		if (plas) { c.plas_x = plas[2 * j]; c.plas_y = plas[2 * j + 1]; }
+		if (d_plas_w) c.plas_w = d_plas_w + (size_t)j * nwave * 2;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
 		if (post(pcol_->col(c, s), "GPUMultislice column pass")) return 401;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
@@ -679,15 +720,22 @@ int JmsB200::GPUMultislice(int islc0, int accmode, float weight)
 {
 	if (d_wav_ == nullptr || nx_ * ny_ <= 0) return 1;
 	if (!(status_gpu_ & STATUS_CORE)) return 2;
-	if (plasmon_on_) {
-		std::fprintf(stderr, "Error: (GPUMultislice): plasmon Monte-Carlo shifts are not available in this library.\n");
-		return 5;
-	}
 	if (accmode == 0 && ClearDetMem_d() != 0) return 3;
 	const int islc = std::min(std::max(islc0, 0), nobjslc_);
 	std::vector<int> var((size_t)std::max(nobjslc_, 1), 0);
-	if (islc < nobjslc_) GetRandomVariantSequence(var.data()); // a new draw per run
-	int e = run_slices(1, islc, var.data(), weight, d_wav_, nullptr, 0, 0, nullptr, d_detint_, nullptr, 1, 0, 0);
+	std::vector<int> plas;
+	if (islc < nobjslc_) {
+		GetRandomVariantSequence(var.data()); // a new draw per run
+		if (plasmon_on_) { // one Monte-Carlo path per run, after the variant draw
+			pl_nex_ = 0;
+			pl_tqx_ = pl_tqy_ = 0.f;
+			plas.assign(2 * (size_t)nobjslc_, 0);
+			for (int j = islc; j < nobjslc_; j++)
+				plasmon_step(GetSliceThickness(objslc_[j]), &plas[2 * j], &plas[2 * j + 1]);
+		}
+	}
+	int e = run_slices(1, islc, var.data(), weight, d_wav_, nullptr, 0, 0, nullptr, d_detint_, nullptr, 1, 0, 0,
+		plas.empty() ? nullptr : plas.data());
 	if (e) return e;
 	if (imagedet_ & (DET_DIFFR_AVG | DET_IMAGE_AVG)) weight_imgavg_ += weight;
 	if (imagedet_ & (DET_WAVEF_AVG | DET_WAVER_AVG)) weight_wavavg_ += weight;
@@ -954,6 +1002,9 @@ void JmsB200::free_all()
 {
 	if (stream_) cudaStreamSynchronize(stream_);
 	dfree(d_pgr_); dfree(d_pro_); dfree(d_det_); dfree(d_wav0_); dfree(d_wav_); dfree(d_cppl_);
+	dfree(d_plas_);
+	d_plas_ = nullptr;
+	plas_cap_ = 0;
 	dfree(d_detint_); dfree(d_dif_); dfree(d_img_); dfree(d_wff_); dfree(d_wfr_);
 	dfree(d_dif_avg_); dfree(d_img_avg_); dfree(d_wff_avg_); dfree(d_wfr_avg_);
 }
@@ -993,16 +1044,40 @@ int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, co
 	if (post(launch_make_shift(d_shift_, d_pos, npos, a0_[0], a0_[1], fz, stream_), "ScanGPU")) return 1;
 	launches_++;
 	const int B = std::max(1, scan_batch_);
-	std::vector<int> var((size_t)nobjslc_);
+	std::vector<int> var((size_t)nobjslc_), plas_h;
 	const float w = 1.f / (float)npass;
 	for (int p0 = 0; p0 < npos; p0 += B) {
 		const int nw = std::min(B, npos - p0);
 		for (int ip = 0; ip < npass; ip++) {
 			if (varseq) std::memcpy(var.data(), varseq + (size_t)ip * nobjslc_, sizeof(int) * nobjslc_);
 			else GetRandomVariantSequence(var.data());
+			if (plasmon_on_) {
+				// one Monte-Carlo path per wave (positions in order), after the
+				// pass's variant draw; shifts [slice][wave][2] to the device
+				plas_h.assign((size_t)nobjslc_ * nw * 2, 0);
+				for (int iw = 0; iw < nw; iw++) {
+					pl_nex_ = 0;
+					pl_tqx_ = pl_tqy_ = 0.f;
+					for (int j = 0; j < nobjslc_; j++) {
+						int* d = &plas_h[((size_t)j * nw + iw) * 2];
+						plasmon_step(GetSliceThickness(objslc_[j]), d, d + 1);
+					}
+				}
+				if (plas_h.size() > plas_cap_) {
+					dfree(d_plas_);
+					d_plas_ = nullptr;
+					plas_cap_ = 0;
+					if (post(cudaMalloc(&d_plas_, sizeof(int) * plas_h.size()), "ScanGPU")) return 1;
+					plas_cap_ = plas_h.size();
+				}
+				if (post(cudaMemcpyAsync(d_plas_, plas_h.data(), sizeof(int) * plas_h.size(), cudaMemcpyHostToDevice,
+					stream_), "ScanGPU")) return 1;
+			}
 			int e = run_slices(nw, 0, var.data(), w, d_wav0_, d_shift_ + (size_t)p0 * 4, 0, 0, d_cppl_,
 				d_out_int ? d_out_int + (size_t)p0 * ndetslc_ * ndet_ : nullptr,
-				d_out_bin ? d_out_bin + (size_t)p0 * nbx * nby : nullptr, bin, nbx, nby);
+				d_out_bin ? d_out_bin + (size_t)p0 * nbx * nby : nullptr, bin, nbx, nby, nullptr,
+				plasmon_on_ ? d_plas_ : nullptr);
+			if (plasmon_on_ && post(cudaStreamSynchronize(stream_), "ScanGPU")) return 1;   // plas_h reuse
 			if (e) return e;
 		}
 	}

@@ -68,7 +68,8 @@ public:
 	void SetDiffractionDescanN(int whichcode, int ndx, int ndy);
 	void SetDiffractionDescan(int whichcode, float dkx, float dky);
 	void SetDiffractionDescanMRad(int whichcode, float dmx, float dmy);
-	void SetPlasmonMC(bool use, unsigned int nexmax) { plasmon_on_ = (use && nexmax > 0) ? 1 : 0; }
+	// bulk plasmon Monte-Carlo (src/JMultiSlice.cpp:973-981, src/JPlasmonMC.cpp)
+	void SetPlasmonMC(bool use, float q_e, float q_c, float mfp, unsigned int nexmax);
 
 	// ---- generators (host, as in the reference)
 	int CalculateProbeWaveFourier(const ProbeParams& prm, float* wav) const;
@@ -157,7 +158,11 @@ private:
 	int ensure_work(int nwave);
 	int ensure_partial(int nwave);
 	int run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src, const double* d_shift,
-		int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx, int nby);
+		int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx, int nby,
+		const int* plas = nullptr, const int* d_plas_w = nullptr);
+	// one slice of the plasmon Monte-Carlo (CJPlasmonMC::ScatGridMC); returns
+	// the number of new excitations, (di, dj) the change of the pixel shift
+	int plasmon_step(float dt, int* di, int* dj);
 	void free_all();
 
 	// parameters
@@ -207,6 +212,11 @@ private:
 	std::vector<cudaEvent_t> ev_col_, ev_row_;   // start/stop pairs
 	cudaEvent_t timed_event();
 	int plasmon_on_ = 0;
+	float pl_qe_ = 0.f, pl_qc_ = 0.f, pl_mfp_ = 0.f;
+	unsigned int pl_nmax_ = 0, pl_nex_ = 0;
+	float pl_tqx_ = 0.f, pl_tqy_ = 0.f;
+	int* d_plas_ = nullptr;         // per-wave plasmon shifts of a scan chunk [nobj][nwave][2]
+	size_t plas_cap_ = 0;
 	long long launches_ = 0;
 	cudaError_t last_cuda_ = cudaSuccess;
 };

@@ -52,6 +52,11 @@ struct PassArgs {
 	int bin = 1, nbx = 0, nby = 0;
 	int bin_plane = -1;             // plane at which the binned pattern is taken
 	int descan_x = 0, descan_y = 0; // integer-pixel diffraction descan of the Fourier readout
+	// column pass: cyclic shift (plas_x, plas_y) pixels of the spectrum after
+	// the forward transform (plasmon scattering, CShift2d), applied as the
+	// real-space ramp exp(2 pi i (plas_x x / nx + plas_y y / ny)) with x t
+	int plas_x = 0, plas_y = 0;
+	const int* plas_w = nullptr;    // [nwave][2] per-wave shifts of this slice (replaces plas_x / plas_y)
 	int store = 1;                  // row pass: 0 = stop after the readout (last slice)
 	// Band of live Fourier rows: row ky (scrambled index) can be nonzero only
 	// if ky <= k1 or ky >= k2.  Propagators vanish outside their band limit,

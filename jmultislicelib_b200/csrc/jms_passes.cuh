@@ -579,6 +579,19 @@ k_col_pass(const PassArgs p)
 					v[e] = cmul(v[e], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
 				}
 			}
+			int sx = p.plas_x, sy = p.plas_y;
+			if (p.plas_w) { sx = __ldg(p.plas_w + 2 * b); sy = __ldg(p.plas_w + 2 * b + 1); }
+			if (sx | sy) { // plasmon shift of the spectrum (uniform branch)
+				const float tx = (float)(int)(((long long)sx * x) % nx) / (float)nx;
+				#pragma unroll
+				for (int e = 0; e < PL::EMID; e++) {
+					const int y = PL::mid(pos, e);
+					const float ty = (float)(int)(((long long)sy * y) % p.ny) / (float)p.ny;
+					float sn, cs;
+					sincospif(2.f * (tx + ty), &sn, &cs);
+					v[e] = cmul(v[e], make_float2(cs, sn));
+				}
+			}
 		}
 	}
 	PL::template from_mid<false, T>(v, sm, p.twy, tid);

@@ -18,6 +18,7 @@
  *   - probe offset OffsetIncomingWave (CPU branch)        src/JMultiSlice.cpp:1999-2031
  *   - detection plane hash SetDetectionPlanes             src/JMultiSlice.cpp:579-626
  *   - variant draws GetRandomVariantSequence              src/JMultiSlice.cpp:1571-1676
+ *   - plasmon Monte-Carlo shifts CJPlasmonMC::ScatGridMC  src/JPlasmonMC.cpp:153-209
  *     with CRng (std::mt19937 + uniform_int_distribution) src/rng.cpp:30-74
  *   - phase gratings of CJEElaSca (2-D projection mode)   src/JEElaSca.cpp:486-741, 812-976
  *     from radial form-factor tables (linear interpolation as
@@ -233,6 +234,48 @@ int or_variant_sequence(void* rng, int nscslc, const int* nvarslc, int nobjslc, 
 	return 0;
 }
 
+// Bulk plasmon Monte-Carlo path of one multislice run (CJPlasmonMC, src/JPlasmonMC.cpp:
+// 153-209, as GPUMultislice / CPUMultislice draw it after the variant sequence,
+// src/JMultiSlice.cpp:4583-4603, 3650-3690): per object slice j >= islc0 a
+// Poisson number of new excitations (mean dt_j / mfp, float), capped at the
+// remaining budget nexmax; each adds q (q^2 = qe^2 ((qc/qe)^2 + 1)^u - qe^2)
+// in the direction 2 pi u'; the spectrum moves by the change of
+// round(q_total * a) pixels.  shifts [nobjslc][2] (x, y pixels), zero where
+// nothing moves.  The arithmetic is float as in the reference.
+int or_plasmon_shifts(void* rng, int nobjslc, int islc0, const float* dt, float ax, float ay, float q_e,
+	float q_c, float mfp, unsigned int nexmax, int* shifts)
+{
+	OrRng* R = (OrRng*)rng;
+	if (!R || !shifts || !dt) return 2;
+	for (int j = 0; j < 2 * nobjslc; j++) shifts[j] = 0;
+	q_e = std::fabs(q_e); q_c = std::fabs(q_c); mfp = std::fabs(mfp);
+	if (mfp <= 0.f || q_e <= 0.f || q_c < q_e) return 0;
+	const float qe2 = q_e * q_e, qc2 = q_c * q_c;
+	unsigned int nex = 0;
+	float tqx = 0.f, tqy = 0.f;
+	for (int j = (islc0 < 0 ? 0 : islc0); j < nobjslc; j++) {
+		std::poisson_distribution<int> pd((double)(dt[j] / mfp));
+		unsigned int n = (unsigned int)pd(R->urng);
+		if (n > nexmax - nex) n = nexmax - nex;
+		if (n == 0) continue;
+		float qx = 0.f, qy = 0.f;
+		for (unsigned int i = 0; i < n; i++) {
+			const float phi = (float)(kTwoPi * R->unirand(0.0, 1.0));
+			const float u = (float)R->unirand(0.0, 1.0);
+			const float q = std::sqrt(qe2 * std::pow(qc2 / qe2 + 1.f, u) - qe2);
+			qx += q * std::cos(phi);
+			qy += q * std::sin(phi);
+		}
+		const int i0 = (int)std::round(tqx * ax), j0 = (int)std::round(tqy * ay);
+		nex += n;
+		tqx += qx;
+		tqy += qy;
+		shifts[2 * j] = (int)std::round(tqx * ax) - i0;
+		shifts[2 * j + 1] = (int)std::round(tqy * ay) - j0;
+	}
+	return 0;
+}
+
 // OffsetIncomingWave, CPU branch (src/JMultiSlice.cpp:1999-2031), in FP64:
 // out(k) = wav0(k - tilt) * exp(-i [2 pi (kx dx + ky dy + k^2 dz wl/2) + cppl(k)]).
 // kx = fnx(i)/a, ky = fny(j)/b with the scrambled frequency numbers of
@@ -275,7 +318,7 @@ int or_multislice(int nx, int ny, double* wav, int nobjslc, int islc0,
 	const float* pro, const int* pro_idx, const int* det_objslc,
 	int ndet, const float* det, const int* msklen, const int* msk,
 	int imagedet, double weight,
-	double* det_int, double* dif, double* img, double* wff, double* wfr)
+	double* det_int, double* dif, double* img, double* wff, double* wfr, const int* shifts)
 {
 	const long N = (long)nx * ny;
 	zd* w = reinterpret_cast<zd*>(wav);
@@ -333,6 +376,13 @@ int or_multislice(int nx, int ny, double* wav, int nobjslc, int islc0,
 			}
 		}
 		fft2d(w, nx, ny, -1);
+		if (shifts && (shifts[2 * j] || shifts[2 * j + 1])) { // plasmon: cyclic shift of the spectrum (CShift2d)
+			std::vector<zd> t(w, w + N);
+			const int sx = imod(shifts[2 * j], nx), sy = imod(shifts[2 * j + 1], ny);
+			for (int y = 0; y < ny; y++)
+				for (int x = 0; x < nx; x++)
+					w[(long)((y + sy) % ny) * nx + (x + sx) % nx] = t[(long)y * nx + x];
+		}
 		const std::complex<float>* P = pr + (long)pro_idx[j] * N;
 		for (long i = 0; i < N; i++) w[i] = cmul(w[i], zd(P[i].real(), P[i].imag()));
 	}

@@ -49,7 +49,10 @@ def lib():
         L.or_offset.argtypes = [_i, _i, _d, _d, _d, _fp, _d, _d, _d, _fp, _i, _i, _dp]
         L.or_offset.restype = None
         L.or_multislice.argtypes = [_i, _i, _dp, _i, _i, _fp, _i, _i, _ip, _fp, _ip, _ip,
-                                    _i, _fp, _ip, _ip, _i, _d, _dp, _dp, _dp, _dp, _dp]
+                                    _i, _fp, _ip, _ip, _i, _d, _dp, _dp, _dp, _dp, _dp, _ip]
+        _f = C.c_float
+        L.or_plasmon_shifts.argtypes = [_p, _i, _i, _fp, _f, _f, _f, _f, _f, C.c_uint, _ip]
+        L.or_plasmon_shifts.restype = _i
         L.or_multislice.restype = _i
         L.or_pgr.argtypes = [_i, _i, _d, _d, _d, _i, _dp, _fp, _ip, _i, _i, _d, _fp, _i, _i, _dp]
         L.or_pgr.restype = _i
@@ -98,6 +101,15 @@ class Rng:
         except Exception:
             pass
 
+    def plasmon_shifts(self, dt, ax, ay, q_e, q_c, mfp, nexmax, islc0=0) -> np.ndarray:
+        """One plasmon Monte-Carlo path (CJPlasmonMC::ScatGridMC per slice) from
+        this generator: [nobjslc, 2] pixel shifts."""
+        d, pd = _f32(dt)
+        out = np.zeros((len(d), 2), np.int32)
+        e = lib().or_plasmon_shifts(self.h, len(d), islc0, pd, ax, ay, q_e, q_c, mfp, nexmax, out.ctypes.data_as(_ip))
+        assert e == 0
+        return out
+
     def variant_sequence(self, nvarslc, objslc) -> np.ndarray:
         """GetRandomVariantSequence (src/JMultiSlice.cpp:1571-1676)."""
         nv, pnv = _i32(nvarslc)
@@ -119,7 +131,7 @@ def offset(wav0, a, b, wl, dx, dy, dz=0.0, cppl=None, ibtx=0, ibty=0) -> np.ndar
 
 
 def multislice(wav, pgr_pool, pgr_idx, pro_pool, pro_idx, det_objslc, ndetslc, det=None, masks=None,
-               imagedet=1, weight=1.0, islc0=0, acc=None):
+               imagedet=1, weight=1.0, islc0=0, acc=None, shifts=None):
     """One CPUMultislice run (src/JMultiSlice.cpp:3589-3720) in FP64.
 
     wav: complex Fourier-space entrance wave [ny, nx] (offset applied).
@@ -127,6 +139,7 @@ def multislice(wav, pgr_pool, pgr_idx, pro_pool, pro_idx, det_objslc, ndetslc, d
     of object slice jslc; pro_pool [m, ny, nx] with pro_idx likewise.
     det: float [ndet, ny, nx]; masks: list of int arrays (empty = no mask).
     acc: dict of accumulators to add into (accmode 1), else fresh zeros.
+    shifts: [nobjslc, 2] plasmon pixel shifts of the spectrum per slice, or None.
     Returns dict with det_int [ndetslc, ndet], dif, img, wff, wfr.
     """
     w = np.ascontiguousarray(wav, np.complex128).copy()
@@ -153,11 +166,12 @@ def multislice(wav, pgr_pool, pgr_idx, pro_pool, pro_idx, det_objslc, ndetslc, d
             "wff": np.zeros((ndetslc, ny, nx), np.complex128),
             "wfr": np.zeros((ndetslc, ny, nx), np.complex128),
         }
+    sh, psh = (None, None) if shifts is None else _i32(np.asarray(shifts).reshape(-1))
     e = lib().or_multislice(nx, ny, w.ctypes.data_as(_dp), nobjslc, islc0, ppg, npgx, npgy, pgi, ppr, pri, pdh,
                             ndet, pdt, pml, pmk, imagedet, weight,
                             acc["det_int"].ctypes.data_as(_dp), acc["dif"].ctypes.data_as(_dp),
                             acc["img"].ctypes.data_as(_dp), acc["wff"].ctypes.data_as(_dp),
-                            acc["wfr"].ctypes.data_as(_dp))
+                            acc["wfr"].ctypes.data_as(_dp), psh)
     assert e == 0
     acc["wave"] = w
     return acc

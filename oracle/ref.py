@@ -85,6 +85,8 @@ def lib():
             "ref_calc_propagator": ([_p, _f, _f, _f, _i, _fp], _i),
             "ref_calc_ring_detector": ([_p, _f, _f, _f, _f, _f, _f, C.c_char_p, _fp, _ip, _ip, _i], _i),
             "ref_cpu_scan": ([C.POINTER(_p), _i, _i, _fp, _i, _i, _fp], _i),
+            "ref_set_slice_thickness": ([_p, _i, _f], None),
+            "ref_set_plasmon": ([_p, _i, _f, _f, _f, C.c_uint], None),
             "ref_readout_det_avg": ([_p, _i, _i, _fp, _fp, _i], _i),
             "ref_pgr": ([_i, _i, _f, _f, _f, _f, _i, _i, _f, _i, _ip, _fp, _fp, _fp, _i, _i, _fp, _ip, _fp, _ip, _fp,
                          _ip, C.POINTER(C.c_double)], _i),
@@ -227,6 +229,12 @@ class RefJMS:
         w = C.c_float(0)
         self.L.ref_get_avg_result(self.h, code, which, dst.view(np.float32).ctypes.data_as(_fp), C.byref(w), ithread)
         return dst, w.value
+
+    def set_slice_thickness(self, islc, t):
+        lib().ref_set_slice_thickness(self.h, islc, t)
+
+    def set_plasmon(self, use, q_e, q_c, mfp, nexmax):
+        lib().ref_set_plasmon(self.h, int(use), q_e, q_c, mfp, nexmax)
 
     def readout_det_avg(self, code, which, count, ithread=0):
         """CJMultiSlice::ReadoutDetAvg: (error, dst, weight)."""

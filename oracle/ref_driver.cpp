@@ -153,6 +153,12 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	return err.load();
 }
 
+void ref_set_slice_thickness(void* h, int islc, float t) { ((RefJMS*)h)->SetSliceThickness(islc, t); }
+void ref_set_plasmon(void* h, int use, float q_e, float q_c, float mfp, unsigned int nexmax)
+{
+	((RefJMS*)h)->SetPlasmonMC(use != 0, q_e, q_c, mfp, nexmax);
+}
+
 // CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.cpp:2667-2945).
 int ref_readout_det_avg(void* h, int whichcode, int whichresult, float* dst, float* weight, int ithread)
 {

@@ -94,7 +94,8 @@ def variant_draws(g):
 
 
 def make_case(g, name, nx, ny, a, b, kv, nvar, objslc, thick, proidx, protype, tilt, dets, ndetper,
-              imagedet, runs, seed, npg=None, probe=(25.0, {}), islc0=0, cppl_seed=None, avg_reads=()):
+              imagedet, runs, seed, npg=None, probe=(25.0, {}), islc0=0, cppl_seed=None, avg_reads=(),
+              plasmon=None, slcthick=None):
     """Set up one reference object (CPU code), run `runs` = [(dx,dy,dz,ibtx,ibty,accmode,weight)]."""
     rng = np.random.default_rng(seed)
     R = ref.RefJMS()
@@ -125,6 +126,11 @@ def make_case(g, name, nx, ny, a, b, kv, nvar, objslc, thick, proidx, protype, t
     if cppl_seed is not None:
         cppl = np.random.default_rng(cppl_seed).uniform(-0.5, 0.5, (ny, nx)).astype(np.float32)
         R.set_phaseplate(CPU, cppl)
+    if slcthick is not None:
+        for s_, t_ in enumerate(slcthick):
+            R.set_slice_thickness(s_, t_)
+    if plasmon is not None:
+        R.set_plasmon(1, *plasmon)
     R.seed(seed)
     for (dx, dy, dz, ibtx, ibty, accmode, w) in runs:
         assert R.offset(CPU, dx, dy, dz, 0, ibtx, ibty) == 0
@@ -151,6 +157,9 @@ def make_case(g, name, nx, ny, a, b, kv, nvar, objslc, thick, proidx, protype, t
         g[p + f"msk{i}"] = m
     if cppl is not None:
         g[p + "cppl"] = cppl
+    if plasmon is not None:
+        g[p + "plasmon"] = np.array(plasmon, np.float32)
+        g[p + "slcthick"] = np.array(slcthick, np.float32)
     g[p + "ndetslc"] = np.int32(nd)
     if imagedet & INT:
         g[p + "det_int"] = R.get_result(CPU, INT, nd * len(dets)).reshape(nd, len(dets))
@@ -204,6 +213,13 @@ def multislice_cases(g):
     make_case(g, "msg", 48, 48, 1.0, 1.0, 300.0, [3, 2], [0, 1] * 5, [0.19525], [0, 0], 1, (0.0, 0.0), ring[:3],
               5, INT | IMG | DIF | WFR_AVG | WFF_AVG,
               [(0.1, 0.2, 0.0, 0, 0, 0, 0.5), (0.3, 0.1, 0.0, 0, 0, 1, 0.25), (0.2, 0.4, 0.0, 0, 0, 1, 0.25)], 29)
+    # H: bulk plasmon Monte-Carlo (short mean free path so that several
+    # excitations happen): q_e, q_c [1/nm], mfp [nm], at most 3 excitations;
+    # four accumulating runs, each its own Monte-Carlo path.
+    make_case(g, "msh", 64, 64, 1.5, 1.5, 300.0, [2, 2], [0, 1] * 8, [0.2], [0, 0], 1, (0.0, 0.0), ring[:3],
+              4, INT | DIF | WFF, [(0.3, 0.4, 0.0, 0, 0, 0, 0.25), (0.3, 0.4, 0.0, 0, 0, 1, 0.25),
+                                  (0.3, 0.4, 0.0, 0, 0, 1, 0.25), (0.3, 0.4, 0.0, 0, 0, 1, 0.25)], 31,
+              plasmon=(0.8, 6.0, 0.6, 3), slcthick=[0.2, 0.2])
     # E: start slice > 0, probe beam tilt in pixels and a constant phase plate.
     make_case(g, "mse", 64, 64, 1.2, 1.2, 300.0, [2, 2], [0, 1] * 5, [0.19525], [0, 0], 1, (0.0, 0.0), ring[:3],
               3, INT | DIF | IMG, [(0.2, 0.1, 0.5, 2, -1, 0, 1.0)], 21, islc0=4, cppl_seed=3)

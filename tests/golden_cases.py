@@ -17,7 +17,7 @@ _cache = None
 
 INT, IMG, DIF, WFR, WFF = 1, 2, 4, 8, 16
 IMG_AVG, DIF_AVG, WFR_AVG, WFF_AVG = 32, 64, 128, 256
-CASES = ("msa", "msb", "msc", "msd", "mse", "msf", "msg")
+CASES = ("msa", "msb", "msc", "msd", "mse", "msf", "msg", "msh")
 
 
 def golden():
@@ -59,12 +59,17 @@ def oracle_case(name: str) -> dict:
     for (dx, dy, dz, ibtx, ibty, accmode, w) in c["runs"]:
         var = rng.variant_sequence(c["nvar"], c["objslc"])
         pidx = (base[c["objslc"]] + var).astype(np.int32)
+        shifts = None
+        if "plasmon" in c and c["islc0"] < nobj:   # one Monte-Carlo path per run, after the variant draw
+            qe, qc, mfp, nmax = (float(v) for v in c["plasmon"])
+            shifts = rng.plasmon_shifts(c["slcthick"][c["objslc"]], np.float32(c["a"]), np.float32(c["b"]), qe, qc,
+                                        mfp, int(nmax), islc0=c["islc0"])
         wav = OR.offset(c["probe"], c["a"], c["b"], c["wl"], dx, dy, dz, c.get("cppl"), int(ibtx), int(ibty))
         if accmode == 0 or acc is None:
             acc = None
         res = OR.multislice(wav, pool, pidx, np.stack(c["pro"]), c["proidx"][c["objslc"]], hsh, ndetslc,
                             det=det, masks=c["msk"], imagedet=c["imagedet"], weight=float(w),
-                            islc0=c["islc0"], acc=acc)
+                            islc0=c["islc0"], acc=acc, shifts=shifts)
         acc = res
         # averaging channels are never cleared by accmode 0 (src/JMultiSlice.cpp:3128-3166)
         if c["imagedet"] & (IMG_AVG | DIF_AVG | WFR_AVG | WFF_AVG):
@@ -73,7 +78,7 @@ def oracle_case(name: str) -> dict:
                 avg["w"] = 0.0
             one = OR.multislice(wav, pool, pidx, np.stack(c["pro"]), c["proidx"][c["objslc"]], hsh, ndetslc,
                                 det=det, masks=c["msk"], imagedet=c["imagedet"], weight=float(w),
-                                islc0=c["islc0"])
+                                islc0=c["islc0"], shifts=shifts)
             for k in avg:
                 if k != "w":
                     avg[k] += one[k]

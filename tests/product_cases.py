@@ -26,6 +26,13 @@ def setup_case(J, c):
     assert J.set_incident_wave(GPU, c["probe"]) == 0
     if "cppl" in c:
         assert J.set_phaseplate(GPU, c["cppl"]) == 0
+    if "plasmon" in c:
+        for s_, t_ in enumerate(c["slcthick"]):
+            J.L.SetSliceThickness(s_, float(t_))
+        qe, qc, mfp, nmax = (float(v) for v in c["plasmon"])
+        J.L.SetPlasmonMC(1, qe, qc, mfp, int(nmax))
+    else:
+        J.L.SetPlasmonMC(0, 0.0, 0.0, 0.0, 0)
 
 
 def run_case(J, name):

@@ -235,12 +235,44 @@ def test_descan_shifts_readout(J):
     assert det_rel(di1, expect_int) < 1e-5
 
 
-def test_plasmon_request_fails_loudly(J):
-    c = G.case("msd")
+def test_scan_with_plasmon_paths(J):
+    """Batched scan with the plasmon Monte-Carlo: every wave of every pass
+    draws its own path (positions in order, after the pass's variant draw)."""
+    from oracle import oracle as OR
+
+    c = G.case("msh")
     PC.setup_case(J, c)
-    J.L.SetPlasmonMC(1, 1.0, 1.0, 100.0, 2)
+    nx, ny = c["nx"], c["ny"]
+    nobj = len(c["objslc"])
+    pos = np.array([[0.1, 0.2], [0.5, 0.3], [0.9, 1.1]], np.float32)
+    npass = 2
+    orng = OR.Rng(5)
+    varseq = np.stack([orng.variant_sequence(c["nvar"], c["objslc"]) for _ in range(npass)])
+    J.seed(44)
+    J.L.JMS_SetScanBatch(2)          # chunks of 2 and 1 waves
     try:
-        J.offset(GPU, 0.0, 0.0, 0.0)
-        assert J.gpu_multislice(0, 0, 1.0) == 5
+        e, out, _ = J.scan(pos, npass, varseq=varseq)
     finally:
+        J.L.JMS_SetScanBatch(32)
         J.L.SetPlasmonMC(0, 0.0, 0.0, 0.0, 0)
+    assert e == 0
+    qe, qc, mfp, nmax = (float(v) for v in c["plasmon"])
+    rng = OR.Rng(44)
+    paths = {}
+    for p0 in range(0, len(pos), 2):
+        for ip in range(npass):
+            for iw in range(p0, min(p0 + 2, len(pos))):
+                paths[(iw, ip)] = rng.plasmon_shifts(c["slcthick"][c["objslc"]], np.float32(c["a"]),
+                                                     np.float32(c["b"]), qe, qc, mfp, int(nmax))
+    assert any(paths[k].any() for k in paths)
+    n, hsh = OR.detection_planes(c["ndetper"], nobj)
+    base = np.concatenate([[0], np.cumsum(c["nvar"])[:-1]]).astype(np.int64)
+    for iw in range(len(pos)):
+        acc = None
+        for ip in range(npass):
+            w0 = OR.offset(c["probe"], c["a"], c["b"], c["wl"], float(pos[iw, 0]), float(pos[iw, 1]))
+            acc = OR.multislice(w0, np.concatenate(c["pgr"]), (base[c["objslc"]] + varseq[ip]).astype(np.int32),
+                                np.stack(c["pro"]), c["proidx"][c["objslc"]], hsh, n, det=np.stack(c["det"]),
+                                masks=c["msk"], imagedet=G.INT, weight=1.0 / npass, acc=acc,
+                                shifts=paths[(iw, ip)])
+        assert det_rel(out[iw], acc["det_int"][:, :c["ndet"]]) < TOL
