@@ -206,6 +206,38 @@ int JMS_GridSupported(int nx, int ny);
  * 1 for the CPU code, or 21-23 / 121-122 on device errors. */
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight);
 
+/* ---- EMS slice files (.sli) ----------------------------------------------
+ * Phase-grating files of Dr. Probe / EMS as the reference's bench driver reads
+ * them (test/JMSBench1/prm_slice_file_info.h:60-150, prm_slice_file_info.cpp
+ * load_ems_header, prm_slice.cpp load_ems_data): 8192-byte header, nvar
+ * complex64 gratings [nvar][ny][nx] at data_offset.  Files of the other byte
+ * order are detected (first word outside [0, 16384]) and swapped on input. */
+typedef struct JMSSliHeader {
+	int nx, ny;                 /* grid */
+	int nvar;                   /* number of variants (1 for old header versions) */
+	int content;                /* 0 phase grating, 1 potential */
+	unsigned int version;       /* extended header version */
+	unsigned int data_offset;   /* byte offset of the gratings */
+	unsigned int table_offset;  /* byte offset of the atom table */
+	float thickness;            /* slice thickness [nm] */
+	float ekv;                  /* beam energy [keV] */
+	float sx, sy;               /* slice size [nm] */
+	int swapped;                /* 1 if the file has the other byte order */
+	char title[41];             /* slice title (40 chars + NUL) */
+} JMSSliHeader;
+/* Returns 0, 1 (bad arguments), 2 (cannot open), 3 (short header), 4 (invalid header). */
+int JMS_SliReadHeader(const char* path, JMSSliHeader* hdr);
+/* Reads the nvar gratings into pgr (2 * nx * ny * nvar floats); 5 = short data. */
+int JMS_SliReadData(const char* path, float* pgr);
+/* Writes a slice file (header version 2020052801, data at 8192, empty atom
+ * table) from hdr (nx, ny, nvar, content, thickness, ekv, sx, sy, title) and
+ * pgr; 6 = write error. */
+int JMS_SliWrite(const char* path, const JMSSliHeader* hdr, const float* pgr);
+/* Loads a slice file's gratings as the variants of structure slice islc of
+ * the GPU setup (SetSlicePhaseGratings); 7 = grid of the file differs from
+ * the grating grid of PhaseGratingSetup. */
+int JMS_SliLoadSlice(const char* path, int islc);
+
 /* ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273) --------
  * The 2-D projection mode of CJEElaSca::CalculatePhasegratingGPU
  * (src/JEElaSca.cpp:978-1159) run on the device: Fourier synthesis of the

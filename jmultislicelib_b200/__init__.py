@@ -34,6 +34,14 @@ class JMSProbeParams(C.Structure):
                 ("m_fspread_kernel_width", _f), ("m_fspread_kernel_samples", _i), ("m_abrr_coeff", _fp)]
 
 
+class JMSSliHeader(C.Structure):
+    """EMS slice-file header fields (include/jms_b200.h)."""
+
+    _fields_ = [("nx", _i), ("ny", _i), ("nvar", _i), ("content", _i), ("version", C.c_uint),
+                ("data_offset", C.c_uint), ("table_offset", C.c_uint), ("thickness", _f), ("ekv", _f), ("sx", _f),
+                ("sy", _f), ("swapped", _i), ("title", C.c_char * 41)]
+
+
 # name -> (argtypes, restype) of every symbol declared in include/jms_b200.h
 SIGNATURES = {
     "GetJMSVersion": ([], _f), "SetJMSDebugLevel": ([_i], _i), "SeedRngEx": ([_i], None),
@@ -70,6 +78,10 @@ SIGNATURES = {
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
     "JMS_ReadoutDetAvg": ([_i, _i, _fp, _fp], _i),
+    "JMS_SliReadHeader": ([C.c_char_p, C.POINTER(JMSSliHeader)], _i),
+    "JMS_SliReadData": ([C.c_char_p, _fp], _i),
+    "JMS_SliWrite": ([C.c_char_p, C.POINTER(JMSSliHeader), _fp], _i),
+    "JMS_SliLoadSlice": ([C.c_char_p, _i], _i),
     "JMS_PgrSetup": ([_i, _i, _f, _f, _f, _i, _i, _i], _i),
     "JMS_PgrSetFormFactors": ([_i, _i, _f, _fp, _fp], _i),
     "JMS_PgrCalculate": ([_i, _fp, _f, _i, C.c_ulonglong, _i, _i, _fp], _i),
@@ -106,6 +118,32 @@ def _fptr(a):
 
 def _c64(a):
     return np.ascontiguousarray(a, np.complex64)
+
+
+def sli_read(path):
+    """EMS slice file -> (header dict, gratings complex64 [nvar, ny, nx]) (JMS_SliReadHeader / ReadData)."""
+    h = JMSSliHeader()
+    e = lib().JMS_SliReadHeader(os.fsencode(path), C.byref(h))
+    if e:
+        raise OSError(f"JMS_SliReadHeader({path}) returned {e}")
+    d = {k: getattr(h, k) for k, _ in JMSSliHeader._fields_}
+    d["title"] = h.title.decode("latin-1").rstrip("\x00 ")
+    pgr = np.zeros((h.nvar, h.ny, h.nx), np.complex64)
+    e = lib().JMS_SliReadData(os.fsencode(path), _fptr(pgr))
+    if e:
+        raise OSError(f"JMS_SliReadData({path}) returned {e}")
+    return d, pgr
+
+
+def sli_write(path, pgr, thickness, ekv, sx, sy, title="", content=0):
+    """Writes gratings [nvar, ny, nx] as an EMS slice file (JMS_SliWrite)."""
+    g = np.ascontiguousarray(pgr, np.complex64)
+    if g.ndim == 2:
+        g = g[None]
+    h = JMSSliHeader(nx=g.shape[2], ny=g.shape[1], nvar=g.shape[0], content=content, thickness=thickness, ekv=ekv,
+                     sx=sx, sy=sy)
+    h.title = title.encode("latin-1")[:40]
+    return lib().JMS_SliWrite(os.fsencode(path), C.byref(h), _fptr(g))
 
 
 class JMS:
@@ -230,6 +268,9 @@ class JMS:
     # additions
     def set_stream(self, stream_ptr):
         return self.L.JMS_SetStream(C.c_void_p(stream_ptr))
+
+    def sli_load_slice(self, path, islc):
+        return self.L.JMS_SliLoadSlice(os.fsencode(path), islc)
 
     # ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273)
     def pgr_setup(self, nx, ny, a, b, ekv, thermal=0, bwl_pot=0, bwl_pgr=1):

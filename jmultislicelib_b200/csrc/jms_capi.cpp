@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 #include <thread>
+#include <vector>
 
 using jms::JmsB200;
 
@@ -172,6 +173,19 @@ int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::
 
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight)
 { return J().ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }
+
+int JMS_SliLoadSlice(const char* path, int islc)
+{
+	JMSSliHeader h;
+	int e = JMS_SliReadHeader(path, &h);
+	if (e) return e;
+	int npgx = 0, npgy = 0;
+	if (J().GratingSlot(islc, 0, 1, &npgx, &npgy) == nullptr) return 1;
+	if (h.nx != npgx || h.ny != npgy) return 7;
+	std::vector<float> buf((size_t)2 * h.nx * h.ny * h.nvar);
+	if ((e = JMS_SliReadData(path, buf.data()))) return e;
+	return J().SetPhaseGratingData(jms::CODE_GPU, islc, h.nvar, buf.data());
+}
 
 int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int bwl_pot, int bwl_pgr)
 {

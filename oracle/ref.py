@@ -87,6 +87,8 @@ def lib():
             "ref_cpu_scan": ([C.POINTER(_p), _i, _i, _fp, _i, _i, _fp], _i),
             "ref_set_slice_thickness": ([_p, _i, _f], None),
             "ref_set_plasmon": ([_p, _i, _f, _f, _f, C.c_uint], None),
+            "ref_sli_read_header": ([C.c_char_p, _ip, C.POINTER(C.c_ulonglong), _fp, C.c_char_p], _i),
+            "ref_sli_write": ([C.c_char_p, _i, _i, _i, _i, _f, _f, _f, _f, C.c_char_p, _fp], _i),
             "ref_readout_det_avg": ([_p, _i, _i, _fp, _fp, _i], _i),
             "ref_pgr": ([_i, _i, _f, _f, _f, _f, _i, _i, _f, _i, _ip, _fp, _fp, _fp, _i, _i, _fp, _ip, _fp, _ip, _fp,
                          _ip, C.POINTER(C.c_double)], _i),
@@ -314,3 +316,25 @@ def pgr(nx, ny, a, b, c, ekv, Z, biso, occ, pos, thermal=0, absorb=0, abf=0.0, n
         torch.set_num_threads(nt0)
     assert e == 0, e
     return out, at, ff[:nt.value, :nk.value].copy(), sk.value, sec.value
+
+
+def sli_read_header(path):
+    """The bench driver's prm_slice_file_info::load_ems_header on a file."""
+    ints = np.zeros(5, np.int32)
+    offs = (C.c_ulonglong * 2)()
+    f = np.zeros(4, np.float32)
+    title = C.create_string_buffer(41)
+    e = lib().ref_sli_read_header(os.fsencode(path), iptr(ints), offs, fptr(f), title)
+    assert e == 0, e
+    return {"nx": int(ints[0]), "ny": int(ints[1]), "nvar": int(ints[2]), "content": int(ints[3]),
+            "version": int(ints[4]) & 0xFFFFFFFF, "data_offset": int(offs[0]), "table_offset": int(offs[1]),
+            "thickness": float(f[0]), "ekv": float(f[1]), "sx": float(f[2]), "sy": float(f[3]),
+            "title": title.value.decode("latin-1")}
+
+
+def sli_write(path, pgr, thickness, ekv, sx, sy, title="", content=0):
+    """A slice file whose header is written by prm_slice_file_info::save_ems_header."""
+    g = np.ascontiguousarray(pgr, np.complex64)
+    e = lib().ref_sli_write(os.fsencode(path), g.shape[2], g.shape[1], g.shape[0], content, thickness, ekv, sx, sy,
+                            title.encode("latin-1"), fptr(g))
+    assert e == 0, e

@@ -14,11 +14,13 @@
  */
 #include "JMultiSlice.h"
 #include "JEElaSca.h"
+#include "prm_slice_file_info.h"
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <dlfcn.h>
 #include <thread>
+#include <fstream>
 #include <vector>
 #include <string>
 #include <cstring>
@@ -157,6 +159,44 @@ void ref_set_slice_thickness(void* h, int islc, float t) { ((RefJMS*)h)->SetSlic
 void ref_set_plasmon(void* h, int use, float q_e, float q_c, float mfp, unsigned int nexmax)
 {
 	((RefJMS*)h)->SetPlasmonMC(use != 0, q_e, q_c, mfp, nexmax);
+}
+
+// EMS slice-file header through the bench driver's prm_slice_file_info
+// (test/JMSBench1/prm_slice_file_info.cpp): load_ems_header of a file, and a
+// file whose header comes from save_ems_header (data appended at 8192).
+// ints: nx, ny, nvar, content, version; offs: data, table; f: thickness, ekv, sx, sy.
+int ref_sli_read_header(const char* path, int* ints, unsigned long long* offs, float* f, char* title)
+{
+	prm_slice_file_info h;
+	std::ifstream fs(path, std::ios::binary);
+	if (!fs.is_open()) return 2;
+	int e = h.load_ems_header(&fs);
+	if (e) return e;
+	ints[0] = (int)h.grid_x; ints[1] = (int)h.grid_y; ints[2] = (int)h.num_var; ints[3] = (int)h.data_type;
+	ints[4] = (int)h.ver;
+	offs[0] = h.data_offset; offs[1] = h.structure_offset;
+	f[0] = h.sz; f[1] = h.ekv; f[2] = h.sx; f[3] = h.sy;
+	std::memcpy(title, h.s_slc_name, 40);
+	return 0;
+}
+
+int ref_sli_write(const char* path, int nx, int ny, int nvar, int content, float thickness, float ekv, float sx,
+	float sy, const char* title, const float* pgr)
+{
+	prm_slice_file_info h;
+	h.grid_x = (unsigned)nx; h.grid_y = (unsigned)ny; h.num_var = (unsigned)nvar; h.data_type = (unsigned)content;
+	h.data_offset = 8192; h.structure_offset = 0x1100;
+	h.sz = thickness; h.ekv = ekv; h.sx = sx; h.sy = sy;
+	std::memset(h.s_slc_name, 0, 40);
+	std::strncpy(h.s_slc_name, title, 40);
+	std::ofstream fs(path, std::ios::binary);
+	if (!fs.is_open()) return 2;
+	int e = h.save_ems_header(&fs);
+	if (e) return e;
+	std::vector<char> pad(8192 - 0x1100, 0);
+	fs.write(pad.data(), pad.size());
+	fs.write((const char*)pgr, sizeof(float) * 2 * (size_t)nx * ny * nvar);
+	return fs.good() ? 0 : 6;
 }
 
 // CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.cpp:2667-2945).

@@ -276,3 +276,25 @@ def test_scan_with_plasmon_paths(J):
                                 masks=c["msk"], imagedet=G.INT, weight=1.0 / npass, acc=acc,
                                 shifts=paths[(iw, ip)])
         assert det_rel(out[iw], acc["det_int"][:, :c["ndet"]]) < TOL
+
+def test_slice_files_load_into_setup(J, tmp_path):
+    """Gratings loaded from EMS slice files (JMS_SliLoadSlice) run exactly as
+    the same gratings uploaded with SetSlicePhaseGratings."""
+    import jmultislicelib_b200 as jb
+
+    c, ref_out = PC.run_case(J, "msb")
+    PC.setup_case(J, c)
+    for s, gr in enumerate(c["pgr"]):
+        p = str(tmp_path / f"msb_{s + 1:03d}.sli")
+        assert jb.sli_write(p, gr, 0.2, c["kv"], c["a"], c["b"]) == 0
+        assert J.sli_load_slice(p, s) == 0
+    J.seed(c["seed"])
+    for (dx, dy, dz, ibtx, ibty, accmode, w) in c["runs"]:
+        assert J.offset(GPU, float(dx), float(dy), float(dz), 0, int(ibtx), int(ibty)) == 0
+        assert J.gpu_multislice(c["islc0"], int(accmode), float(w)) == 0
+    nd = J.num_det_planes()
+    di = J.get_result(GPU, G.INT, nd * c["ndet"]).reshape(nd, c["ndet"])
+    np.testing.assert_array_equal(di, ref_out["det_int"])
+    p = str(tmp_path / "wrong_001.sli")
+    assert jb.sli_write(p, np.ones((1, 8, 8), np.complex64), 0.2, 300.0, 1.0, 1.0) == 0
+    assert J.sli_load_slice(p, 0) == 7
