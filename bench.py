@@ -452,6 +452,142 @@ def reference_grating_cpu(cfg):
                       f"CJEElaSca::CalculatePhasegratingCPU, {total:.2f} s"}
 
 
+# Uneven batch: 12 specimens cycling through 256, 384, 512, 720 and 1024 grid
+# points, 50-400 slices, 1-16 phonon variants, scans of 16x16 to 64x64
+# (numpy PCG64, seed 20261206); ABO3 supercells of n / 64 cells, gratings
+# made on the device (JMS_PgrCalculate, QEP variants).  A step is one raster
+# row of every specimen (one phonon pass), i.e. sum(nscan * nobj) multislice
+# steps over all 12 grids.
+UNEVEN_SEED = 20261206
+
+
+def uneven_specimens():
+    rng = np.random.default_rng(UNEVEN_SEED)
+    out = []
+    for i in range(12):
+        n = (256, 384, 512, 720, 1024)[i % 5]
+        out.append({"n": n, "nobj": int(rng.integers(50, 401)), "nvar": int(rng.integers(1, 17)),
+                    "nscan": int(rng.choice([16, 32, 48, 64])), "ncell": n // 64})
+    return out
+
+
+def run_uneven(args):
+    import ctypes as C
+
+    import torch
+
+    import jmultislicelib_b200 as jb
+    from jmultislicelib_b200 import synthetic as S
+
+    torch.cuda.set_device(0)
+    J = jb.JMS()
+    specs = uneven_specimens()
+    ctxs, rows = [], []
+    t_gen = 0.0
+    for k, sp in enumerate(specs):
+        cid = J.L.JMS_CreateContext()
+        ctxs.append(cid)
+        J.L.JMS_SelectContext(cid)
+        n, nc = sp["n"], sp["ncell"]
+        a = nc * S.A_CELL
+        J.set_high_tension(300.0)
+        J.set_grid(n, n, a, a, S.DZ_SLICE)
+        pro = J.calc_propagator(S.DZ_SLICE, 0.0, 0.0, 1)
+        dets = [J.calc_ring_detector(b0, b1) for (b0, b1) in ((0, 10), (20, 50), (80, 200))]
+        abrr = np.zeros(48, np.float32)
+        abrr[10] = 1000.0
+        probe = J.calc_probe(22.0, abrr=abrr)
+        objslc = np.arange(sp["nobj"]) % 2
+        assert J.setup(2, [sp["nvar"]] * 2, objslc, [0, 0], 20, 3, 1) == [0, 0, 0, 0]
+        ff, sk = S.form_factor_tables(n, n, a, a, UNEVEN_SEED + k)
+        assert J.pgr_setup(n, n, a, a, 300.0, 2, 0, 1) == 0
+        assert J.pgr_set_form_factors(ff, sk, [S.BISO_PHONON] * 3) == 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s_ in range(2):
+            e, _ = J.pgr_calculate(S.layer_atoms(nc, nc, s_), S.DZ_SLICE, ngr=sp["nvar"], seed=k * 10 + s_,
+                                   islc=s_, ivar0=0, want=False)
+            assert e == 0, e
+        torch.cuda.synchronize()
+        t_gen += time.perf_counter() - t0
+        assert J.set_propagator(2, 0, pro) == 0
+        for i, (d, m) in enumerate(dets):
+            assert J.set_detector(2, i, d, m) == 0
+        assert J.init_core(2) == 0
+        assert J.set_incident_wave(2, probe) == 0
+        J.seed(100 + k)
+        J.L.JMS_SetScanBatch(64)
+        mid = (nc // 2) * S.A_CELL
+        pos = S.scan_positions(sp["nscan"], mid, mid, S.A_CELL)[:sp["nscan"]]   # one raster row
+        d_pos = torch.from_numpy(np.ascontiguousarray(pos)).cuda()
+        d_out = torch.zeros((len(pos), J.num_det_planes(), 3), dtype=torch.float64, device="cuda")
+        rows.append((d_pos, d_out))
+    steps = sum(sp["nscan"] * sp["nobj"] for sp in specs)
+
+    def enqueue(k):
+        J.L.JMS_SelectContext(ctxs[k])
+        d_pos, d_out = rows[k]
+        e = J.L.JMS_ScanGPUDevice(d_pos.shape[0], d_pos.data_ptr(), 0.0, 1, None, d_out.data_ptr(), None, 0)
+        assert e == 0, e
+
+    def sequential():
+        for k in range(len(specs)):
+            enqueue(k)
+            torch.cuda.synchronize()
+
+    def concurrent():
+        for k in range(len(specs)):
+            enqueue(k)
+        torch.cuda.synchronize()
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    reps = max(1, args.steps)
+    res = {}
+    for cid in ctxs:                       # fixed schedule: each length's default plan
+        J.L.JMS_SelectContext(cid)
+        J.L.JMS_SelectPlans(0, 0)
+    res["fixed_sequential"] = timed(sequential, reps)
+    tuned = {}
+    for k, cid in enumerate(ctxs):         # autotuned plans per grid
+        J.L.JMS_SelectContext(cid)
+        ir, ic = C.c_int(0), C.c_int(0)
+        assert J.L.JMS_Autotune(min(64, specs[k]["nscan"]), 10, None, None, C.byref(ir), C.byref(ic)) == 0
+        buf = C.create_string_buffer(64)
+        J.L.JMS_PlanName(0, buf, 64)
+        tuned[specs[k]["n"]] = buf.value.decode()
+    res["tuned_sequential"] = timed(sequential, reps)
+    res["tuned_concurrent"] = timed(concurrent, reps)
+    arr = np.array(ctxs, np.int32)
+    assert J.L.JMS_GraphBegin(len(ctxs), arr.ctypes.data_as(C.POINTER(C.c_int))) == 0
+    for k in range(len(specs)):
+        enqueue(k)
+    h = J.L.JMS_GraphEnd()
+    assert h >= 1, h
+    res["tuned_graph"] = timed(lambda: J.L.JMS_GraphLaunch(h, None, 1), reps)
+    J.L.JMS_GraphDestroy(h)
+    J.L.JMS_SelectContext(0)
+    for cid in ctxs:
+        J.L.JMS_DestroyContext(cid)
+    line = {"metric": "uneven batch multislice steps/s", "value": steps / res["tuned_graph"], "unit": "steps/s",
+            "n_gpus": 1, "steps": reps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "12 specimens (256-1024 grid points, 50-400 slices, 1-16 QEP variants), "
+                                   "one raster row each, one phonon pass", "specimens": specs,
+                       "multislice_steps_per_step": steps, "tuned_row_plans": tuned},
+            "modes_steps_per_s": {k: steps / v for k, v in res.items()},
+            "ms_per_step": {k: 1e3 * v for k, v in res.items()},
+            "grating_generation_s": t_gen}
+    print(json.dumps(line))
+    return 0
+
+
 def traffic_from_profiles(kind):
     """DRAM bytes per launch of the pass, from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", f"{kind}_pass_512.md")
@@ -528,9 +664,13 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-err", action="store_true")
+    ap.add_argument("--workload", default="scan", choices=["scan", "uneven"],
+                    help="scan: the headline 512^2 scan; uneven: 12 specimens of uneven grid sizes")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "uneven":
+        return run_uneven(args)
     return run_ours(args)
 
 

@@ -206,6 +206,32 @@ int JMS_GridSupported(int nx, int ny);
  * 1 for the CPU code, or 21-23 / 121-122 on device errors. */
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight);
 
+/* ---- contexts and CUDA graphs -------------------------------------------
+ * A context is one library instance (grid, setup, device buffers, stream) --
+ * what a separate CJMultiSlice object is in the reference's C++ interface.
+ * Context 0 is the default one behind the flat functions; JMS_CreateContext
+ * returns the id of a new one, JMS_SelectContext(id) directs the flat calls
+ * of the calling host thread to it (returns the previous id, -1 for an
+ * unknown id), JMS_DestroyContext(id) frees it (id > 0).  Contexts of
+ * different grid sizes run their scans concurrently: each works on its own
+ * stream (created by InitCore), and JMS_ScanGPUDevice only enqueues. */
+int JMS_CreateContext(void);
+int JMS_SelectContext(int id);
+int JMS_DestroyContext(int id);
+/* Stream capture of the work that the listed contexts enqueue between
+ * JMS_GraphBegin and JMS_GraphEnd into one CUDA graph (fork / join over the
+ * contexts' streams).  JMS_GraphEnd returns a handle >= 1 (negative on
+ * failure).  A graph replays exactly the captured work: kernel arguments,
+ * variant sequences and the device buffers they read, whose contents the
+ * caller may refresh between launches (positions); synchronous calls,
+ * buffer growth, pass timing and plasmon draws are not allowed while
+ * capturing, so run each workload once before capturing it.
+ * JMS_GraphLaunch(handle, stream or NULL, wait). */
+int JMS_GraphBegin(int nctx, const int* ctx);
+int JMS_GraphEnd(void);
+int JMS_GraphLaunch(int handle, void* stream, int wait);
+int JMS_GraphDestroy(int handle);
+
 /* ---- EMS slice files (.sli) ----------------------------------------------
  * Phase-grating files of Dr. Probe / EMS as the reference's bench driver reads
  * them (test/JMSBench1/prm_slice_file_info.h:60-150, prm_slice_file_info.cpp

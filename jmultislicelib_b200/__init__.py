@@ -78,6 +78,9 @@ SIGNATURES = {
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
     "JMS_ReadoutDetAvg": ([_i, _i, _fp, _fp], _i),
+    "JMS_CreateContext": ([], _i), "JMS_SelectContext": ([_i], _i), "JMS_DestroyContext": ([_i], _i),
+    "JMS_GraphBegin": ([_i, _ip], _i), "JMS_GraphEnd": ([], _i), "JMS_GraphLaunch": ([_i, _p, _i], _i),
+    "JMS_GraphDestroy": ([_i], _i),
     "JMS_SliReadHeader": ([C.c_char_p, C.POINTER(JMSSliHeader)], _i),
     "JMS_SliReadData": ([C.c_char_p, _fp], _i),
     "JMS_SliWrite": ([C.c_char_p, C.POINTER(JMSSliHeader), _fp], _i),

@@ -9,15 +9,37 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
 using jms::JmsB200;
 
+// Library contexts: context 0 is the default instance of the reference's flat
+// interface; JMS_CreateContext adds more (each with its own grid, setup,
+// device buffers and stream), and JMS_SelectContext picks the one the flat
+// calls of the calling host thread act on.
+namespace {
+std::mutex g_ctx_mu;
+std::vector<std::unique_ptr<JmsB200>> g_ctx;
+thread_local int t_ctx = 0;
+
+JmsB200* ctx_get(int id)
+{
+	if (g_ctx.empty()) g_ctx.emplace_back(new JmsB200());
+	return (id >= 0 && id < (int)g_ctx.size()) ? g_ctx[id].get() : nullptr;
+}
+} // namespace
+
 static JmsB200& J()
 {
-	static std::unique_ptr<JmsB200> inst(new JmsB200());
-	return *inst;
+	std::lock_guard<std::mutex> lock(g_ctx_mu);
+	JmsB200* j = ctx_get(t_ctx);
+	if (j == nullptr) {
+		t_ctx = 0;
+		j = ctx_get(0);
+	}
+	return *j;
 }
 
 static jms::PgrGen& G()
@@ -174,6 +196,132 @@ int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight)
 { return J().ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }
 
+int JMS_CreateContext(void)
+{
+	std::lock_guard<std::mutex> lock(g_ctx_mu);
+	ctx_get(0);
+	for (size_t i = 1; i < g_ctx.size(); i++)
+		if (!g_ctx[i]) { g_ctx[i].reset(new JmsB200()); return (int)i; }
+	g_ctx.emplace_back(new JmsB200());
+	return (int)g_ctx.size() - 1;
+}
+
+int JMS_SelectContext(int id)
+{
+	std::lock_guard<std::mutex> lock(g_ctx_mu);
+	if (ctx_get(id) == nullptr) return -1;
+	const int old = t_ctx;
+	t_ctx = id;
+	return old;
+}
+
+int JMS_DestroyContext(int id)
+{
+	std::unique_ptr<JmsB200> victim;
+	{
+		std::lock_guard<std::mutex> lock(g_ctx_mu);
+		if (id <= 0 || ctx_get(id) == nullptr) return 1;
+		victim = std::move(g_ctx[id]);
+		if (t_ctx == id) t_ctx = 0;
+	}
+	return 0;   // the context is freed here, outside the lock
+}
+
+// ---- CUDA graphs over contexts -------------------------------------------
+namespace {
+struct GraphRec {
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+};
+std::mutex g_graph_mu;
+std::vector<std::unique_ptr<GraphRec>> g_graphs;
+cudaStream_t g_origin = nullptr;
+std::vector<cudaStream_t> g_cap_streams;
+bool g_capturing = false;
+} // namespace
+
+int JMS_GraphBegin(int nctx, const int* ctx)
+{
+	std::lock_guard<std::mutex> lock(g_graph_mu);
+	if (g_capturing || nctx < 1 || ctx == nullptr) return 1;
+	std::vector<cudaStream_t> streams;
+	{
+		std::lock_guard<std::mutex> lk(g_ctx_mu);
+		for (int i = 0; i < nctx; i++) {
+			JmsB200* j = ctx_get(ctx[i]);
+			if (j == nullptr) return 1;
+			if (j->Stream() == nullptr) return 2;   // the context needs its stream (InitCore)
+			for (cudaStream_t q : streams)
+				if (q == j->Stream()) return 1;
+			streams.push_back(j->Stream());
+		}
+	}
+	if (g_origin == nullptr && cudaStreamCreateWithFlags(&g_origin, cudaStreamNonBlocking) != cudaSuccess) return 3;
+	if (cudaStreamBeginCapture(g_origin, cudaStreamCaptureModeRelaxed) != cudaSuccess) return 3;
+	cudaEvent_t fork;
+	cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+	cudaEventRecord(fork, g_origin);
+	for (cudaStream_t q : streams) cudaStreamWaitEvent(q, fork, 0);
+	cudaEventDestroy(fork);
+	g_cap_streams = streams;
+	g_capturing = true;
+	return 0;
+}
+
+int JMS_GraphEnd(void)
+{
+	std::lock_guard<std::mutex> lock(g_graph_mu);
+	if (!g_capturing) return -1;
+	g_capturing = false;
+	for (cudaStream_t q : g_cap_streams) {
+		cudaEvent_t join;
+		cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+		cudaEventRecord(join, q);
+		cudaStreamWaitEvent(g_origin, join, 0);
+		cudaEventDestroy(join);
+	}
+	g_cap_streams.clear();
+	std::unique_ptr<GraphRec> r(new GraphRec());
+	if (cudaStreamEndCapture(g_origin, &r->graph) != cudaSuccess || r->graph == nullptr) {
+		cudaGetLastError();
+		return -2;
+	}
+	if (cudaGraphInstantiate(&r->exec, r->graph, 0) != cudaSuccess) {
+		cudaGraphDestroy(r->graph);
+		cudaGetLastError();
+		return -3;
+	}
+	for (size_t i = 0; i < g_graphs.size(); i++)
+		if (!g_graphs[i]) { g_graphs[i] = std::move(r); return (int)i + 1; }
+	g_graphs.push_back(std::move(r));
+	return (int)g_graphs.size();
+}
+
+int JMS_GraphLaunch(int handle, void* stream, int wait)
+{
+	cudaGraphExec_t x = nullptr;
+	{
+		std::lock_guard<std::mutex> lock(g_graph_mu);
+		if (handle < 1 || handle > (int)g_graphs.size() || !g_graphs[handle - 1]) return 1;
+		x = g_graphs[handle - 1]->exec;
+	}
+	cudaStream_t s = stream ? (cudaStream_t)stream : g_origin;
+	if (cudaGraphLaunch(x, s) != cudaSuccess) return 2;
+	if (wait && cudaStreamSynchronize(s) != cudaSuccess) return 3;
+	return 0;
+}
+
+int JMS_GraphDestroy(int handle)
+{
+	std::lock_guard<std::mutex> lock(g_graph_mu);
+	if (handle < 1 || handle > (int)g_graphs.size() || !g_graphs[handle - 1]) return 1;
+	GraphRec* r = g_graphs[handle - 1].get();
+	cudaGraphExecDestroy(r->exec);
+	cudaGraphDestroy(r->graph);
+	g_graphs[handle - 1].reset();
+	return 0;
+}
+
 int JMS_SliLoadSlice(const char* path, int islc)
 {
 	JMSSliHeader h;
@@ -205,8 +353,13 @@ int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned 
 		dst = J().GratingSlot(islc, ivar0, ngr, &npgx, &npgy);
 		if (dst == nullptr || npgx != G().nx() || npgy != G().ny()) return 9;
 	}
-	G().SetStream(J().Stream());
-	return G().Calculate(natom, atoms, cz, ngr, seed, dst, pgr);
+	cudaStream_t s = J().Stream();
+	G().SetStream(s);
+	int e = G().Calculate(natom, atoms, cz, ngr, seed, dst, pgr);
+	// before InitCore the context has no stream of its own yet, and the one it
+	// creates does not wait for the legacy stream: finish the gratings here
+	if (e == 0 && dst != nullptr && s == nullptr && cudaStreamSynchronize(nullptr) != cudaSuccess) e = 7;
+	return e;
 }
 
 } // extern "C"
