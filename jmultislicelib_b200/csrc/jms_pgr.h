@@ -7,14 +7,14 @@
 //             with ff2d_type(q) = f_type(|q|) [ap1(q)], f linearly
 //             interpolated from the radial table (CAtomType::GetFormFactor,
 //             src/Atoms.cpp:414-436), ap1 the smooth potential band limit
-//             (src/JEElaSca.cpp:590-593), applied twice as the reference does
-//             (PrepareScatteringFunctions :733-741 and the add :905-913);
+//             (src/JEElaSca.cpp:597-600), applied twice as the reference does
+//             (PrepareScatteringFunctions :738-739 and the add :934);
 //   V'(r)   = IFT[pot] (unscaled, e^{+i});
 //   t(r)    = exp(i c V'(r)),  c = lambda cz / (4 pi vol): the reference's
 //             POT_SCA / vol and PGR_SIG cz lambda, whose constant product is
-//             1 / (4 pi) (src/JEElaSca.cpp:944-950, JEElaSca.h:88-94);
+//             1 / (4 pi) (src/JEElaSca.cpp:947, 956-963, JEElaSca.h:88-94);
 //   t       = IFT[ FT[t] ap2 ],  ap2 = 1/(nx ny) for |q| <= 2/3 kmax, else 0
-//             (m_bwl_pgr, :956-960, aperture :595-602).
+//             (m_bwl_pgr, :965-969, aperture :602-609).
 //
 // Design: one synthesis kernel per batch of gratings (every grating a new
 // draw of the site displacements in the quantum-excitation-of-phonons model,

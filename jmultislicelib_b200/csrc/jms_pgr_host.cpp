@@ -84,7 +84,7 @@ int PgrGen::SetGrid(int nx, int ny, float a, float b)
 	twiddles(tw, ny);
 	if (cudaMalloc(&d_twy_, sizeof(float2) * ny) != cudaSuccess) return 4;
 	cudaMemcpy(d_twy_, tw.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice);
-	// phase-grating aperture (src/JEElaSca.cpp:575-602): 1/(nx ny) inside
+	// phase-grating aperture (src/JEElaSca.cpp:586-609): 1/(nx ny) inside
 	// 2/3 of the smaller Nyquist frequency, 0 outside; float arithmetic as there
 	const int nx2 = (nx - nx % 2) >> 1, ny2 = (ny - ny % 2) >> 1;
 	const float itogx = 1.f / a, itogy = 1.f / b;
@@ -113,7 +113,7 @@ int PgrGen::SetPhysics(float ekv, int thermal, int bwl_pot, int bwl_pgr)
 	thermal_ = thermal;
 	bwl_pot_ = bwl_pot ? 1 : 0;
 	bwl_pgr_ = bwl_pgr ? 1 : 0;
-	// electron wavelength as CJEElaSca computes it (src/JEElaSca.cpp:827), float
+	// electron wavelength as CJEElaSca computes it (src/JEElaSca.cpp:826), float
 	const float wlelkev = (float)(kC0 * kHPL / kQEL * 1.0E+6);
 	const float eel0kev = (float)(kME0 * kC0 * kC0 / kQEL / 1000.);
 	wl_ = wlelkev / std::sqrt(ekv * (ekv + 2.f * eel0kev));

@@ -398,14 +398,14 @@ int or_multislice(int nx, int ny, double* wav, int nobjslc, int islc0,
 // (src/JEElaSca.cpp:812-976) in FP64:
 //   pot(q) = sum_atoms occ ff_type(|q|) ap1(q)^2 exp(-2 pi i (fx fi + fy fj))
 //            (ap1 = 0.5 - 0.5 tanh((|q| / kmax - 0.9) 30) if bwl_pot, else 1;
-//             src/JEElaSca.cpp:590-593, applied in PrepareScatteringFunctions
-//             :733-741 and again in the add :905-913)
+//             src/JEElaSca.cpp:597-600, applied in PrepareScatteringFunctions
+//             :738-739 and again in the add :934)
 //   V'(r)  = backward transform of pot (unscaled)
 //   t      = exp(i c V'),  c = wl cz / (4 pi vol) with vol = a b cz: the
-//            reference's POT_SCA / vol and PGR_SIG cz wl (:939-950), whose
+//            reference's POT_SCA / vol and PGR_SIG cz wl (:947, 956-963), whose
 //            constant product is 1 / (4 pi)
 //   bwl_pgr: t = backward[ forward[t] * ap2 ], ap2 = 1 / (nx ny) for
-//            |q| <= 2/3 kmax, 0 beyond (:595-602, :956-960).
+//            |q| <= 2/3 kmax, 0 beyond (:602-609, :965-969).
 // atoms: [natom][2] fractional positions (x / a, y / b) as used (sites,
 // displaced or not); occ [natom]; type [natom]; ff [ntype][nk] complex float.
 int or_pgr(int nx, int ny, double a, double b, double wl, int natom, const double* pos, const float* occ,
