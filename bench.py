@@ -316,14 +316,19 @@ def run_ours(args):
     e2e_step()
     torch.cuda.synchronize()
     barrier()
-    e2e_each = []
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        t1 = time.perf_counter()
-        e2e_step()            # returns after its device work and the result copy
-        e2e_each.append(1e3 * (time.perf_counter() - t1))
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_each, e2e_dev = [], []
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(e2e_steps)]
+    with ClockSampler(local) as clk_e2e:
+        t0 = time.perf_counter()
+        for k in range(e2e_steps):
+            t1 = time.perf_counter()
+            evs[k][0].record(stream)
+            e2e_step()            # returns after its device work and the result copy
+            evs[k][1].record(stream)
+            e2e_each.append(1e3 * (time.perf_counter() - t1))
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    e2e_dev = [a.elapsed_time(b) for a, b in evs]
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -360,6 +365,7 @@ def run_ours(args):
                            "l2": f"inputs larger than L2 (128 MiB grating pool, {2 * waves} MiB of waves per "
                                  "batch, 126 MB L2)"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "ms_each": [round(v, 2) for v in e2e_each],
+                        "device_ms_each": [round(v, 2) for v in e2e_dev], "clocks": clk_e2e.summary(),
                         "h2d_bytes_per_step": int(h_pos.numel() * 4),
                         "d2h_bytes_per_step": int(h_int.numel() * 4 + h_bin.numel() * 4)},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
