@@ -597,6 +597,105 @@ def run_uneven(args):
     return 0
 
 
+# Control-variate frozen-phonon averaging on the headline scan's specimen:
+# ground truth = the mean over 64 phonon configurations at an 8x8 subset of
+# the 64x64 raster; estimator = 4 full configurations + the surrogate on all
+# 64; surrogate trained on pairs from separate configurations and positions.
+def run_cv(args):
+    import torch
+
+    import jmultislicelib_b200 as jb
+    from jmultislicelib_b200 import surrogate as SG
+    from jmultislicelib_b200 import synthetic as S
+
+    torch.cuda.set_device(0)
+    cfg = S.SCAN_512
+    J = jb.JMS()
+    t_spec = time.perf_counter()
+    sp = S.make_specimen(cfg["nx"], cfg["ny"], cfg["ncell"], cfg["ncell"], cfg["nslice_types"], cfg["nvar"],
+                         cfg["seed"], cfg["kv"], keep_potential=True)
+    t_spec = time.perf_counter() - t_spec
+    J.L.JMS_SetScanBatch(64)
+    _, probe, pro, dets, raster = S.setup_library(J, cfg, specimen=sp)
+    nd = J.num_det_planes()
+    planes = list(range(1, nd))                 # the 10 readout thicknesses after the entrance plane
+    nout = len(planes) * len(dets)
+    cell0 = (cfg["ncell"] // 2) * S.A_CELL
+    rng = np.random.default_rng(20261207)
+
+    def configs(n):
+        """n phonon configurations: a random variant of its structure slice per object slice."""
+        return rng.integers(0, cfg["nvar"], (n, cfg["nobj"])).astype(np.int32)
+
+    # training pairs: separate configurations and random positions in the scanned cell
+    tr_cfg = configs(args.cv_train_configs)
+    tr_pos = (cell0 + rng.uniform(0, S.A_CELL, (args.cv_train_positions, 2))).astype(np.float32)
+    d_tr = torch.from_numpy(tr_pos).cuda()
+    X, Y = [], []
+    t_gen = 0.0
+    for v in tr_cfg:
+        maps = SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v)
+        X.append(SG.patches(maps, tr_pos, sp.a, sp.b).astype(np.float32))
+        y, dt = SG.timed(lambda: SG.signals(J, d_tr, len(tr_pos), v, planes))
+        Y.append(y)
+        t_gen += dt
+    # the surrogate learns the phonon fluctuation at a fixed position: inputs
+    # and targets are deviations from their mean over the configurations
+    X = np.stack(X)                    # [config, position, 3, 64, 64]
+    Y = np.stack(Y)                    # [config, position, nout]
+    X -= X.mean(axis=0, keepdims=True)
+    Y -= Y.mean(axis=0, keepdims=True)
+    nval = max(2, len(tr_cfg) // 8)    # held-out configurations: early stopping and beta
+    Xt, Yt = X[nval:].reshape(-1, *X.shape[2:]), Y[nval:].reshape(-1, nout)
+    Xv, Yv = X[:nval].reshape(-1, *X.shape[2:]), Y[:nval].reshape(-1, nout)
+    cv = SG.ControlVariate(nout, batch=256, seed=1)
+    hist, t_train = SG.timed(lambda: cv.fit(Xt, Yt, Xv, Yv, epochs=args.cv_epochs))
+    # evaluation: 8x8 subset of the raster, 64 fresh configurations
+    ev_pos = np.ascontiguousarray(raster.reshape(64, 64, 2)[::8, ::8].reshape(-1, 2))
+    d_ev = torch.from_numpy(ev_pos).cuda()
+    ev_cfg = configs(64)
+    F = np.zeros((64, len(ev_pos), nout))
+    G = np.zeros_like(F)
+    P = np.zeros((64, len(ev_pos), 3, SG.PATCH, SG.PATCH), np.float32)
+    t_full = t_sur = t_patch = 0.0
+    for k, v in enumerate(ev_cfg):
+        F[k], dt = SG.timed(lambda: SG.signals(J, d_ev, len(ev_pos), v, planes))
+        t_full += dt
+        t0 = time.perf_counter()
+        P[k] = SG.patches(SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v), ev_pos, sp.a, sp.b)
+        t_patch += time.perf_counter() - t0
+    P -= P.mean(axis=0, keepdims=True)
+    G, t_sur = SG.timed(lambda: cv.predict(P.reshape(-1, *P.shape[2:])).reshape(F.shape))
+    truth = F.mean(axis=0)
+    n_few = 4
+    plain = F[:n_few].mean(axis=0)
+    est = SG.cv_estimate(F[:n_few], G[:n_few], G, cv.beta)
+    scale = np.abs(truth).mean(axis=0)[None, :]
+    e_plain = np.sqrt((((plain - truth) / scale) ** 2).mean(axis=0)).reshape(len(planes), len(dets))
+    e_cv = np.sqrt((((est - truth) / scale) ** 2).mean(axis=0)).reshape(len(planes), len(dets))
+    var_f = F.var(axis=0).mean(axis=0)
+    var_r = (F - cv.beta * G).var(axis=0).mean(axis=0)
+    ratio = (var_r / np.maximum(var_f, 1e-300)).reshape(len(planes), len(dets))
+    line = {"metric": "control-variate frozen-phonon estimate", "unit": "relative RMS error", "n_gpus": 1,
+            "data": "synthetic",
+            "config": {"workload": "512^2 scan specimen, 8x8 positions, 64 phonon configurations as ground truth, "
+                                   "estimator 4 full + surrogate on 64",
+                       "train_pairs": int(Xt.shape[0]), "validation_pairs": int(Xv.shape[0]),
+                       "epochs": args.cv_epochs, "outputs": nout},
+            "err_plain4_per_det": [float(v) for v in e_plain.mean(axis=0)],
+            "err_cv4_per_det": [float(v) for v in e_cv.mean(axis=0)],
+            "var_ratio_per_det": [float(v) for v in ratio.mean(axis=0)],
+            "var_ratio_by_thickness": ratio.tolist(),
+            "plain_configs_for_same_error": [float(n_few * (a / max(b, 1e-30)) ** 2)
+                                             for a, b in zip(e_plain.mean(axis=0), e_cv.mean(axis=0))],
+            "loss_train_val_first_last": [hist[0], hist[-1]], "beta_mean": float(np.mean(cv.beta)),
+            "seconds": {"specimen_potentials": t_spec, "training_signals": t_gen, "training": t_train,
+                        "full_multislice_64": t_full, "full_multislice_4": t_full * n_few / 64,
+                        "surrogate_inference_64": t_sur, "patch_inputs_64_host": t_patch}}
+    print(json.dumps(line))
+    return 0
+
+
 def traffic_from_profiles(kind):
     """DRAM bytes per launch of the pass, from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", f"{kind}_pass_512.md")
@@ -673,13 +772,19 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-err", action="store_true")
-    ap.add_argument("--workload", default="scan", choices=["scan", "uneven"],
-                    help="scan: the headline 512^2 scan; uneven: 12 specimens of uneven grid sizes")
+    ap.add_argument("--workload", default="scan", choices=["scan", "uneven", "cv"],
+                    help="scan: the headline 512^2 scan; uneven: 12 specimens of uneven grid sizes; "
+                         "cv: control-variate frozen-phonon averaging with the learned surrogate")
+    ap.add_argument("--cv-train-configs", type=int, default=32)
+    ap.add_argument("--cv-train-positions", type=int, default=625)
+    ap.add_argument("--cv-epochs", type=int, default=30)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "uneven":
         return run_uneven(args)
+    if args.workload == "cv":
+        return run_cv(args)
     return run_ours(args)
 
 

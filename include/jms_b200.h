@@ -264,6 +264,34 @@ int JMS_SliWrite(const char* path, const JMSSliHeader* hdr, const float* pgr);
  * the grating grid of PhaseGratingSetup. */
 int JMS_SliLoadSlice(const char* path, int islc);
 
+/* ---- control-variate surrogate network (no counterpart in the reference) ---
+ * Building blocks of the small convolutional surrogate used as a control
+ * variate for frozen-phonon averaging (jmultislicelib_b200/surrogate.py):
+ * BF16 activations and weights, FP32 accumulation, FP32 gradients.  All
+ * pointers are device pointers, stream may be NULL.  Layouts: activations
+ * [B][C][H][W], conv weights [Co][Ci][3][3] (3x3, stride 2, padding 1),
+ * linear weights [O][C].  Return 0, or 2 for bad arguments, 1 for a launch
+ * error. */
+int JMS_NnConvForward(const void* x, const void* w, const float* bias, void* y, int B, int Ci, int H, int W, int Co,
+	int relu, void* stream);
+/* Backward of JMS_NnConvForward from dL/dy (before the ReLU mask, which is
+ * taken from the stored output y): dx (may be NULL), dw, db. */
+int JMS_NnConvBackward(const void* x, const void* w, const void* y, const float* dy, float* dx, float* dw, float* db,
+	int B, int Ci, int H, int W, int Co, int relu, void* stream);
+/* out[b][o] = bl[o] + sum_c wl[o][c] * mean over HW of h[b][c] (h BF16). */
+int JMS_NnPoolLinearForward(const void* h, const float* wl, const float* bl, float* out, int B, int C, int HW, int O,
+	void* stream);
+int JMS_NnPoolLinearBackward(const void* h, const float* wl, const float* dout, float* dh, float* dwl, float* dbl,
+	int B, int C, int HW, int O, void* stream);
+/* Mean squared error over n values: dout = 2 (out - target) / n, *loss (may
+ * be NULL) = mean (out - target)^2. */
+int JMS_NnMseLoss(const float* out, const float* target, float* dout, float* loss, int n, void* stream);
+/* One Adam step (step >= 1) on FP32 parameters p with moments m, v; writes a
+ * BF16 copy to p_bf16 when given. */
+int JMS_NnAdam(float* p, const float* g, float* m, float* v, void* p_bf16, int n, float lr, float b1, float b2,
+	float eps, int step, void* stream);
+int JMS_NnCastBf16(const float* src, void* dst, long long n, void* stream);
+
 /* ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273) --------
  * The 2-D projection mode of CJEElaSca::CalculatePhasegratingGPU
  * (src/JEElaSca.cpp:978-1159) run on the device: Fourier synthesis of the

@@ -81,6 +81,13 @@ SIGNATURES = {
     "JMS_CreateContext": ([], _i), "JMS_SelectContext": ([_i], _i), "JMS_DestroyContext": ([_i], _i),
     "JMS_GraphBegin": ([_i, _ip], _i), "JMS_GraphEnd": ([], _i), "JMS_GraphLaunch": ([_i, _p, _i], _i),
     "JMS_GraphDestroy": ([_i], _i),
+    "JMS_NnConvForward": ([_p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _p], _i),
+    "JMS_NnConvBackward": ([_p, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _p], _i),
+    "JMS_NnPoolLinearForward": ([_p, _p, _p, _p, _i, _i, _i, _i, _p], _i),
+    "JMS_NnPoolLinearBackward": ([_p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _p], _i),
+    "JMS_NnMseLoss": ([_p, _p, _p, _p, _i, _p], _i),
+    "JMS_NnAdam": ([_p, _p, _p, _p, _p, _i, _f, _f, _f, _f, _i, _p], _i),
+    "JMS_NnCastBf16": ([_p, _p, C.c_longlong, _p], _i),
     "JMS_SliReadHeader": ([C.c_char_p, C.POINTER(JMSSliHeader)], _i),
     "JMS_SliReadData": ([C.c_char_p, _fp], _i),
     "JMS_SliWrite": ([C.c_char_p, C.POINTER(JMSSliHeader), _fp], _i),

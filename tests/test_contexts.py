@@ -54,6 +54,7 @@ def _scan_device(J, pos, varseq, npass, d_out):
     import torch
 
     d_pos = torch.from_numpy(pos).cuda()
+    torch.cuda.synchronize()   # the library stream does not wait for torch's
     vs = np.ascontiguousarray(varseq, np.int32)
     e = J.L.JMS_ScanGPUDevice(len(pos), d_pos.data_ptr(), 0.0, npass, vs.ctypes.data_as(C.POINTER(C.c_int)),
                               d_out.data_ptr(), None, 0)
@@ -88,6 +89,8 @@ def test_contexts_hold_independent_setups(J):
 
 
 def test_uneven_scans_run_concurrently_and_replay_as_a_graph(J):
+    import ctypes as C
+
     import torch
 
     grids = [(256, 256, 12, 3), (384, 384, 8, 2), (128, 96, 16, 4)]
@@ -104,6 +107,7 @@ def test_uneven_scans_run_concurrently_and_replay_as_a_graph(J):
             J.L.JMS_SelectContext(cid)
             nd, ndet = J.num_det_planes(), 3
             d = torch.zeros((len(pos), nd, ndet), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()   # the contexts work on their own streams
             e, _ = _scan_device(J, pos, vs, 2, d)
             assert e == 0
             torch.cuda.synchronize()
@@ -112,11 +116,14 @@ def test_uneven_scans_run_concurrently_and_replay_as_a_graph(J):
         keep = []
         for cid, (pos, vs) in zip(ids, setups):
             J.L.JMS_SelectContext(cid)
-            d = torch.zeros((len(pos), J.num_det_planes(), 3), dtype=torch.float64, device="cuda")
-            e, dp = _scan_device(J, pos, vs, 2, d)
-            assert e == 0
-            outs.append(d)
-            keep.append(dp)
+            outs.append(torch.zeros((len(pos), J.num_det_planes(), 3), dtype=torch.float64, device="cuda"))
+            keep.append(torch.from_numpy(pos).cuda())
+        torch.cuda.synchronize()
+        for cid, (pos, vs), d, dp in zip(ids, setups, outs, keep):
+            J.L.JMS_SelectContext(cid)
+            vsa = np.ascontiguousarray(vs, np.int32)
+            assert J.L.JMS_ScanGPUDevice(len(pos), dp.data_ptr(), 0.0, 2, vsa.ctypes.data_as(C.POINTER(C.c_int)),
+                                         d.data_ptr(), None, 0) == 0
         torch.cuda.synchronize()
         for a, b in zip(outs, seq):
             np.testing.assert_array_equal(a.cpu().numpy(), b)
@@ -125,8 +132,6 @@ def test_uneven_scans_run_concurrently_and_replay_as_a_graph(J):
             d.zero_()
         torch.cuda.synchronize()
         arr = np.array(ids, np.int32)
-        import ctypes as C
-
         assert J.L.JMS_GraphBegin(len(ids), arr.ctypes.data_as(C.POINTER(C.c_int))) == 0
         for cid, (pos, vs), d, dp in zip(ids, setups, outs, keep):
             J.L.JMS_SelectContext(cid)
