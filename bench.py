@@ -696,6 +696,105 @@ def run_cv(args):
     return 0
 
 
+# The headline scan in the quantum-excitation-of-phonons form: every phonon
+# pass gets its own configuration, i.e. 200 freshly displaced gratings (one
+# per object slice) made on the device, instead of draws from a fixed pool
+# of 16 variants per slice type.  The grating store holds one slot per object
+# slice (variant k of type s = the k-th object slice of that type).
+def run_qep(args):
+    import ctypes as C
+
+    import torch
+
+    import jmultislicelib_b200 as jb
+    from jmultislicelib_b200 import synthetic as S
+
+    torch.cuda.set_device(0)
+    cfg = dict(S.SCAN_512)
+    J = jb.JMS()
+    stream = torch.cuda.Stream()
+    J.set_stream(stream.cuda_stream)
+    J.L.JMS_SetScanBatch(args.batch)
+    nobj, nst = cfg["nobj"], cfg["nslice_types"]
+    objslc = np.arange(nobj) % nst
+    count = [int((objslc == s_).sum()) for s_ in range(nst)]
+    rank = np.zeros(nobj, np.int32)
+    for s_ in range(nst):
+        rank[objslc == s_] = np.arange(count[s_])
+    nx, ny, nc = cfg["nx"], cfg["ny"], cfg["ncell"]
+    a = nc * S.A_CELL
+    J.cleanup()
+    J.set_high_tension(cfg["kv"])
+    J.set_grid(nx, ny, a, a, S.DZ_SLICE)
+    pro = J.calc_propagator(S.DZ_SLICE, 0.0, 0.0, cfg["ntype"])
+    dets = [J.calc_ring_detector(b0, b1) for (b0, b1) in cfg["dets"]]
+    abrr = np.zeros(48, np.float32)
+    abrr[10] = cfg["cs"]
+    probe = J.calc_probe(cfg["alpha"], abrr=abrr)
+    assert J.setup(2, count, objslc, [0] * nst, cfg["ndetper"], len(dets), 1) == [0, 0, 0, 0]
+    assert J.set_propagator(2, 0, pro) == 0
+    for i, (d, m) in enumerate(dets):
+        assert J.set_detector(2, i, d, m) == 0
+    assert J.init_core(2) == 0
+    assert J.set_incident_wave(2, probe) == 0
+    ff, sk = S.form_factor_tables(nx, ny, a, a, cfg["seed"], cfg["kv"])
+    assert J.pgr_setup(nx, ny, a, a, cfg["kv"], 2, 0, 1) == 0
+    assert J.pgr_set_form_factors(ff, sk, [S.BISO_PHONON] * 3) == 0
+    layers = [S.layer_atoms(nc, nc, s_ % 2) for s_ in range(nst)]
+    mid = (nc // 2) * S.A_CELL
+    pos = S.scan_positions(cfg["nscan"], mid, mid, S.A_CELL)
+    npos = cfg["nscan"]
+    d_pos = torch.from_numpy(pos[:npos].copy()).cuda()
+    d_int = torch.zeros((npos, J.num_det_planes(), len(dets)), dtype=torch.float64, device="cuda")
+    vs = np.ascontiguousarray(rank, np.int32)
+    vsp = vs.ctypes.data_as(C.POINTER(C.c_int))
+    t_gen = [0.0]
+
+    def one_pass(seed):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for s_ in range(nst):        # a fresh configuration: count[s] new gratings per slice type
+            e, _ = J.pgr_calculate(layers[s_], S.DZ_SLICE, ngr=count[s_], seed=seed * 16 + s_, islc=s_, ivar0=0,
+                                   want=False)
+            assert e == 0, e
+        ev1.record(stream)
+        e = J.L.JMS_ScanGPUDevice(npos, d_pos.data_ptr(), 0.0, 1, vsp, d_int.data_ptr(), None, 0)
+        assert e == 0, e
+        return ev0, ev1
+
+    def step(k):
+        evs = [one_pass(1000 * k + p) for p in range(cfg["nvar"])]
+        return evs
+
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            step(k)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gen_ms = 0.0
+    with ClockSampler(0) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            all_ev = []
+            for k in range(args.steps):
+                all_ev += step(args.warmup + k)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    gen_ms = sum(a.elapsed_time(b) for a, b in all_ev)
+    steps_per = npos * cfg["nvar"] * nobj
+    line = {"metric": "multislice steps/s (512² wave), fresh QEP gratings every pass", "unit": "steps/s",
+            "value": args.steps * steps_per / (ms / 1e3), "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "STEM scan row: 64 positions x 16 phonon passes x 200 slices, 512x512; every "
+                                   "pass a new QEP configuration: 200 gratings generated on the device "
+                                   "(sigma 0.08 A, Gaussian form factors, 2/3 band limit)",
+                       "batch_waves": args.batch},
+            "grating_generation_share": gen_ms / ms, "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 def traffic_from_profiles(kind):
     """DRAM bytes per launch of the pass, from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", f"{kind}_pass_512.md")
@@ -772,9 +871,10 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-err", action="store_true")
-    ap.add_argument("--workload", default="scan", choices=["scan", "uneven", "cv"],
+    ap.add_argument("--workload", default="scan", choices=["scan", "uneven", "cv", "qep"],
                     help="scan: the headline 512^2 scan; uneven: 12 specimens of uneven grid sizes; "
-                         "cv: control-variate frozen-phonon averaging with the learned surrogate")
+                         "cv: control-variate frozen-phonon averaging with the learned surrogate; "
+                         "qep: the headline scan with fresh QEP gratings generated on the device every pass")
     ap.add_argument("--cv-train-configs", type=int, default=32)
     ap.add_argument("--cv-train-positions", type=int, default=625)
     ap.add_argument("--cv-epochs", type=int, default=30)
@@ -785,6 +885,8 @@ def main():
         return run_uneven(args)
     if args.workload == "cv":
         return run_cv(args)
+    if args.workload == "qep":
+        return run_qep(args)
     return run_ours(args)
 
 

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 namespace jms {
@@ -57,13 +58,27 @@ void twiddles(std::vector<float2>& tw, int n)
 
 PgrGen::~PgrGen() { Reset(); }
 
+void PgrGen::SiteSet::release()
+{
+	dfree(base); dfree(ux); dfree(uy); dfree(asite); dfree(aocc); dfree(tstart);
+	base = nullptr; ux = uy = nullptr; asite = tstart = nullptr; aocc = nullptr;
+	key.clear();
+}
+
+void PgrGen::ClearSites()
+{
+	if (!sets_.empty() && stream_) cudaStreamSynchronize(stream_);
+	for (SiteSet& t : sets_) t.release();
+	sets_.clear();
+}
+
 void PgrGen::Reset()
 {
-	dfree(d_ff_); dfree(d_twx_); dfree(d_twy_); dfree(d_ap2_); dfree(d_buf_); dfree(d_out_);
-	dfree(d_base_); dfree(d_ux_); dfree(d_uy_); dfree(d_pos_); dfree(d_asite_); dfree(d_aocc_); dfree(d_tstart_);
+	ClearSites();
+	dfree(d_ff_); dfree(d_twx_); dfree(d_twy_); dfree(d_ap2_); dfree(d_buf_); dfree(d_out_); dfree(d_pos_);
 	d_ff_ = nullptr; d_twx_ = d_twy_ = d_ap2_ = d_buf_ = d_out_ = nullptr;
-	d_base_ = d_pos_ = nullptr; d_ux_ = d_uy_ = nullptr; d_asite_ = d_tstart_ = nullptr; d_aocc_ = nullptr;
-	cap_buf_ = cap_out_ = cap_base_ = cap_ux_ = cap_uy_ = cap_pos_ = cap_asite_ = cap_aocc_ = cap_tstart_ = 0;
+	d_pos_ = nullptr;
+	cap_buf_ = cap_out_ = cap_pos_ = 0;
 	status_ = 0;
 	nx_ = ny_ = 0;
 	ntype_ = nk_ = 0;
@@ -74,6 +89,7 @@ int PgrGen::SetGrid(int nx, int ny, float a, float b)
 {
 	if (nx < 1 || ny < 1 || !(a > 0.f) || !(b > 0.f)) return 1;
 	if (!pgr_supported(nx, ny)) return 8;
+	ClearSites();
 	dfree(d_twx_); dfree(d_twy_); dfree(d_ap2_);
 	d_twx_ = d_twy_ = d_ap2_ = nullptr;
 	nx_ = nx; ny_ = ny; a_ = a; b_ = b;
@@ -109,6 +125,7 @@ int PgrGen::SetGrid(int nx, int ny, float a, float b)
 int PgrGen::SetPhysics(float ekv, int thermal, int bwl_pot, int bwl_pgr)
 {
 	if (!(ekv > 0.f) || thermal < 0 || thermal > 2) return 1;
+	ClearSites();
 	ekv_ = ekv;
 	thermal_ = thermal;
 	bwl_pot_ = bwl_pot ? 1 : 0;
@@ -124,6 +141,7 @@ int PgrGen::SetPhysics(float ekv, int thermal, int bwl_pot, int bwl_pgr)
 int PgrGen::SetFormFactors(int ntype, int nk, float sk, const float* ff, const float* biso)
 {
 	if (ntype < 1 || nk < 2 || !(sk > 0.f) || ff == nullptr) return 1;
+	ClearSites();
 	dfree(d_ff_);
 	d_ff_ = nullptr;
 	if (cudaMalloc(&d_ff_, sizeof(float2) * (size_t)ntype * nk) != cudaSuccess) return 4;
@@ -137,8 +155,19 @@ int PgrGen::SetFormFactors(int ntype, int nk, float sk, const float* ff, const f
 	return 0;
 }
 
-int PgrGen::BuildSites(int natom, const float* atoms, float cz)
+int PgrGen::BuildSites(int natom, const float* atoms, float cz, SiteSet** out)
 {
+	*out = nullptr;
+	for (SiteSet& t : sets_) {
+		if ((int)t.key.size() == 5 * natom + 1 && t.key[5 * natom] == cz &&
+			std::memcmp(t.key.data(), atoms, sizeof(float) * 5 * natom) == 0) {
+			t.used = ++use_clock_;
+			*out = &t;
+			nsite_ = t.nsite;
+			natom_ = t.natom;
+			return 0;
+		}
+	}
 	// CStructure::SetAtomSites (src/Structure.cpp:441-491): an atom joins the
 	// first site closer than 0.05 nm, else opens a new one; a site sits at the
 	// occupancy-weighted mean of its atoms, with their occupancy-weighted Biso
@@ -197,14 +226,35 @@ int PgrGen::BuildSites(int natom, const float* atoms, float cz)
 	for (int t = 0; t < ntype_; t++) tstart[t + 1] += tstart[t];
 	nsite_ = nsite;
 	natom_ = natom;
+	// a new set (the least recently used one of eight is replaced)
+	constexpr size_t kMaxSets = 8;
+	SiteSet* set = nullptr;
+	if (sets_.size() < kMaxSets) {
+		sets_.emplace_back();
+		set = &sets_.back();
+	}
+	else {
+		set = &sets_[0];
+		for (SiteSet& t : sets_)
+			if (t.used < set->used) set = &t;
+		if (stream_) cudaStreamSynchronize(stream_);   // its buffers may still be read
+		set->release();
+	}
 	cudaStream_t s = stream_;
+	size_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
 	int e;
-	if ((e = dput(d_base_, cap_base_, base.data(), base.size(), s))) return e;
-	if ((e = dput(d_ux_, cap_ux_, ux.data(), ux.size(), s))) return e;
-	if ((e = dput(d_uy_, cap_uy_, uy.data(), uy.size(), s))) return e;
-	if ((e = dput(d_asite_, cap_asite_, asite.data(), asite.size(), s))) return e;
-	if ((e = dput(d_aocc_, cap_aocc_, aocc.data(), aocc.size(), s))) return e;
-	if ((e = dput(d_tstart_, cap_tstart_, tstart.data(), tstart.size(), s))) return e;
+	if ((e = dput(set->base, c0, base.data(), base.size(), s))) return e;
+	if ((e = dput(set->ux, c1, ux.data(), ux.size(), s))) return e;
+	if ((e = dput(set->uy, c2, uy.data(), uy.size(), s))) return e;
+	if ((e = dput(set->asite, c3, asite.data(), asite.size(), s))) return e;
+	if ((e = dput(set->aocc, c4, aocc.data(), aocc.size(), s))) return e;
+	if ((e = dput(set->tstart, c5, tstart.data(), tstart.size(), s))) return e;
+	set->key.assign(atoms, atoms + 5 * (size_t)natom);
+	set->key.push_back(cz);
+	set->nsite = nsite;
+	set->natom = natom;
+	set->used = ++use_clock_;
+	*out = set;
 	// the host vectors must outlive the asynchronous copies
 	return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 5;
 }
@@ -214,7 +264,8 @@ int PgrGen::Calculate(int natom, const float* atoms, float cz, int ngr, unsigned
 {
 	if ((status_ & 7) != 7) return 1;
 	if (ngr < 1 || natom < 0 || (natom > 0 && atoms == nullptr) || !(cz > 0.f)) return 3;
-	int e = BuildSites(natom, atoms, cz);
+	SiteSet* set = nullptr;
+	int e = BuildSites(natom, atoms, cz, &set);
 	if (e) return e;
 	const long long N = (long long)nx_ * ny_;
 	cudaStream_t s = stream_;
@@ -231,9 +282,9 @@ int PgrGen::Calculate(int natom, const float* atoms, float cz, int ngr, unsigned
 	p.ny = ny_;
 	p.ngr = ngr;
 	p.nsite = nsite_;
-	p.atom_site = d_asite_;
-	p.atom_occ = d_aocc_;
-	p.type_start = d_tstart_;
+	p.atom_site = set->asite;
+	p.atom_occ = set->aocc;
+	p.type_start = set->tstart;
 	p.ntype = ntype_;
 	p.ff = d_ff_;
 	p.nk = nk_;
@@ -248,7 +299,7 @@ int PgrGen::Calculate(int natom, const float* atoms, float cz, int ngr, unsigned
 	p.twy = d_twy_;
 	if (natom > 0) {
 		if ((e = dput(d_pos_, cap_pos_, (const double2*)nullptr, (size_t)ngr * nsite_, s))) return e;
-		if (launch_pgr_sites(d_pos_, d_base_, d_ux_, d_uy_, nsite_, ngr, seed, s) != cudaSuccess) return 6;
+		if (launch_pgr_sites(d_pos_, set->base, set->ux, set->uy, nsite_, ngr, seed, s) != cudaSuccess) return 6;
 		p.site_pos = d_pos_;
 		if (launch_pgr_synth(p, s) != cudaSuccess) return 6;
 		if (launch_pgr_rows_inv(p, s) != cudaSuccess) return 6;

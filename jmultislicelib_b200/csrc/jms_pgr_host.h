@@ -38,7 +38,23 @@ public:
 	int nsite() const { return nsite_; }
 
 private:
-	int BuildSites(int natom, const float* atoms, float cz);
+	// a structure slice prepared on the device: linked sites, atoms ordered by
+	// type; kept for reuse while the setup is unchanged (the QEP form of a scan
+	// regenerates the same slices every pass)
+	struct SiteSet {
+		std::vector<float> key;         // atoms (5 floats each), then cz
+		int nsite = 0, natom = 0;
+		double2* base = nullptr;
+		double *ux = nullptr, *uy = nullptr;
+		int *asite = nullptr, *tstart = nullptr;
+		float* aocc = nullptr;
+		unsigned long long used = 0;
+		void release();
+	};
+	int BuildSites(int natom, const float* atoms, float cz, SiteSet** out);
+	void ClearSites();
+	std::vector<SiteSet> sets_;
+	unsigned long long use_clock_ = 0;
 
 	int status_ = 0;
 	int nx_ = 0, ny_ = 0;
@@ -52,12 +68,8 @@ private:
 	cudaStream_t stream_ = nullptr;
 	float2* d_ff_ = nullptr;
 	float2 *d_twx_ = nullptr, *d_twy_ = nullptr, *d_ap2_ = nullptr, *d_buf_ = nullptr, *d_out_ = nullptr;
-	double2 *d_base_ = nullptr, *d_pos_ = nullptr;
-	double *d_ux_ = nullptr, *d_uy_ = nullptr;
-	int *d_asite_ = nullptr, *d_tstart_ = nullptr;
-	float* d_aocc_ = nullptr;
-	size_t cap_buf_ = 0, cap_out_ = 0, cap_base_ = 0, cap_ux_ = 0, cap_uy_ = 0, cap_pos_ = 0, cap_asite_ = 0,
-		cap_aocc_ = 0, cap_tstart_ = 0;
+	double2* d_pos_ = nullptr;
+	size_t cap_buf_ = 0, cap_out_ = 0, cap_pos_ = 0;
 };
 
 } // namespace jms
