@@ -16,6 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libjms_b200.so")
+APP = os.path.join(HERE, "jmsbench")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,6 +61,14 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    # the reference-bench-compatible STEM driver (apps/jmsbench.cpp) over the C ABI
+    app_src = os.path.join(HERE, "apps", "jmsbench.cpp")
+    if _newer(APP, [app_src, LIB, os.path.join(ROOT, "include", "jms_b200.h")]):
+        cmd = ["g++", "-std=c++17", "-O2", "-o", APP, app_src, f"-I{ROOT}/include", f"-L{HERE}", "-ljms_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"jmsbench build failed:\n{r.stderr[-4000:]}")
     return LIB
 
 
