@@ -193,6 +193,22 @@ int JMS_PlanCount(int n);
 int JMS_PlanName(int axis, char* name, int len);
 /* 1 if both grid lengths are supported by the fused passes. */
 int JMS_GridSupported(int nx, int ny);
+/* Arithmetic of the line transforms (no counterpart in the reference, whose
+ * GPU path is cuFFT in FP32, src/JFFTCUDAcore.cpp:299-336): 0 = FP32 passes
+ * (default); 1 = tensor-core passes, each radix-16/32 stage a DFT-matrix
+ * product with BF16 hi+lo operands and FP32 accumulation; 2 = the same with
+ * FP16 hi+lo operands (power-of-two scaled per tile).  The tensor-core passes
+ * serve the slices without readout on grids whose lengths are 256, 512 or
+ * 1024; readout slices, sub-frame gratings, plasmon shifts and other lengths
+ * run the FP32 passes.  Returns 0, or 1 for a mode out of range. */
+int JMS_SetPrecision(int mode);
+int JMS_GetPrecision(void);
+/* 1 if a tensor-core pass found its matrix products unfinished after its
+ * bounded wait (about a second) since the last call, else 0 (-1 on a CUDA
+ * error); synchronises the library stream and clears the flag. */
+int JMS_TcStatus(void);
+/* Tensor-core pass launches issued by the library so far. */
+long long JMS_TcLaunches(void);
 
 /* Detector readouts of the averaged wave functions: the public method
  * CJMultiSlice::ReadoutDetAvg (src/JMultiSlice.h:935, .cpp:2667-2945), GPU

@@ -77,6 +77,8 @@ SIGNATURES = {
     "JMS_ScanGPUDevice": ([_i, _p, _f, _i, _ip, _p, _p, _i], _i),
     "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
     "JMS_GridSupported": ([_i, _i], _i),
+    "JMS_SetPrecision": ([_i], _i), "JMS_GetPrecision": ([], _i), "JMS_TcStatus": ([], _i),
+    "JMS_TcLaunches": ([], C.c_longlong),
     "JMS_ReadoutDetAvg": ([_i, _i, _fp, _fp], _i),
     "JMS_CreateContext": ([], _i), "JMS_SelectContext": ([_i], _i), "JMS_DestroyContext": ([_i], _i),
     "JMS_GraphBegin": ([_i, _ip], _i), "JMS_GraphEnd": ([], _i), "JMS_GraphLaunch": ([_i, _p, _i], _i),
@@ -276,6 +278,14 @@ class JMS:
         return self.L.Cleanup()
 
     # additions
+    def set_precision(self, mode):
+        """0 = FP32 passes, 1 = tensor-core passes with BF16 hi+lo operands, 2 = with FP16 hi+lo (JMS_SetPrecision)."""
+        return self.L.JMS_SetPrecision(int(mode))
+
+    def tc_status(self):
+        """0, or 1 if a tensor-core pass gave up waiting for its matrix products (JMS_TcStatus)."""
+        return self.L.JMS_TcStatus()
+
     def set_stream(self, stream_ptr):
         return self.L.JMS_SetStream(C.c_void_p(stream_ptr))
 

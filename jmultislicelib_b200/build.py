@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT}/include"]
 SOURCES = ["jms_kernels.cu", "jms_host.cpp", "jms_generators.cpp", "jms_capi.cpp", "jms_noalloc.cu", "jms_pgr.cu",
-           "jms_pgr_host.cpp", "jms_sli.cpp", "jms_nn.cu"] + [f"jms_inst_{k}.cu" for k in range(10)] + [f"jms_pgr_ops_{k}.cu" for k in range(3)]
+           "jms_pgr_host.cpp", "jms_sli.cpp", "jms_nn.cu", "jms_tc.cu"] + [f"jms_inst_{k}.cu" for k in range(10)] + [f"jms_pgr_ops_{k}.cu" for k in range(3)]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -192,6 +192,10 @@ int JMS_PlanName(int axis, char* name, int len)
 	return 0;
 }
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
+int JMS_SetPrecision(int mode) { return J().SetPrecision(mode); }
+int JMS_GetPrecision(void) { return J().GetPrecision(); }
+int JMS_TcStatus(void) { return J().TcStatus(); }
+long long JMS_TcLaunches(void) { return J().TcLaunches(); }
 
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight)
 { return J().ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }

@@ -63,6 +63,7 @@ JmsB200::~JmsB200()
 	dfree(d_work_);
 	dfree(d_partial_);
 	dfree(d_shift_);
+	dfree(d_tcerr_);
 	if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
 
@@ -684,8 +685,16 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		c.out_k2 = pro_k2_[ip];
 		if (plas) { c.plas_x = plas[2 * j]; c.plas_y = plas[2 * j + 1]; }
 		if (d_plas_w) c.plas_w = d_plas_w + (size_t)j * nwave * 2;
+		// tensor-core form for the steps it covers (no image readout, grating of
+		// the grid size, no plasmon shift), else the FP32 pass
+		const bool tc_col = prec_ > 0 && tc_supported(ny_) && c.plane < 0 && !plas && !d_plas_w && npgx_ == nx_ &&
+			npgy_ == ny_;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
-		if (post(pcol_->col(c, s), "GPUMultislice column pass")) return 401;
+		if (tc_col) {
+			if (post(launch_tc_col(c, prec_, d_tcerr_, s), "GPUMultislice column pass (tensor core)")) return 401;
+			tc_launches_++;
+		}
+		else if (post(pcol_->col(c, s), "GPUMultislice column pass")) return 401;
 		if (timing_on_) { ev_col_.push_back(timed_event()); cudaEventRecord(ev_col_.back(), s); }
 		PassArgs r = four;
 		r.mul = d_pro_ + (long long)ip * N;
@@ -695,8 +704,13 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		r.row_k2 = pro_k2_[ip];
 		in_k1 = pro_k1_[ip];
 		in_k2 = pro_k2_[ip];
+		const bool tc_row = prec_ > 0 && tc_supported(nx_) && r.plane < 0 && r.store;
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
-		if (post(prow_->row(r, s), "GPUMultislice row pass")) return 601;
+		if (tc_row) {
+			if (post(launch_tc_row(r, prec_, d_tcerr_, s), "GPUMultislice row pass (tensor core)")) return 601;
+			tc_launches_++;
+		}
+		else if (post(prow_->row(r, s), "GPUMultislice row pass")) return 601;
 		if (timing_on_) { ev_row_.push_back(timed_event()); cudaEventRecord(ev_row_.back(), s); }
 		launches_ += 2;
 	}
@@ -996,6 +1010,28 @@ int JmsB200::Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* ir
 	if (irow) *irow = best_r;
 	if (icol) *icol = best_c;
 	return 0;
+}
+
+int JmsB200::SetPrecision(int mode)
+{
+	if (mode < 0 || mode > 2) return 1;
+	if (mode > 0 && !d_tcerr_) {
+		if (post(cudaMalloc(&d_tcerr_, sizeof(int)), "tensor-core status")) return 2;
+		if (post(cudaMemsetAsync(d_tcerr_, 0, sizeof(int), stream_), "tensor-core status")) return 2;
+	}
+	if (mode > 0 && post(tc_prepare(stream_), "tensor-core tables")) return 2;
+	prec_ = mode;
+	return 0;
+}
+
+int JmsB200::TcStatus()
+{
+	if (!d_tcerr_) return 0;
+	int h = 0;
+	if (post(cudaMemcpyAsync(&h, d_tcerr_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "tensor-core status")) return -1;
+	if (post(cudaStreamSynchronize(stream_), "tensor-core status")) return -1;
+	if (h) cudaMemsetAsync(d_tcerr_, 0, sizeof(int), stream_);
+	return h;
 }
 
 void JmsB200::free_all()

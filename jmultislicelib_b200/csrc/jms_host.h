@@ -151,6 +151,17 @@ public:
 	void SetPassTiming(int on);
 	int PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row);
 	int LastCudaError() const { return (int)last_cuda_; }
+	// Arithmetic of the line transforms: 0 = FP32 passes (default), 1 = tensor-
+	// core passes with BF16 hi+lo operands, 2 = tensor-core passes with FP16
+	// hi+lo operands (jms_tc.cu).  The tensor-core passes run the steps without
+	// readout for line lengths 256, 512 and 1024; readout steps, sub-frame
+	// gratings, plasmon shifts and other lengths keep the FP32 passes.
+	int SetPrecision(int mode);
+	int GetPrecision() const { return prec_; }
+	// 0, or 1 if a tensor-core pass reported an MMA wait that ran out (the
+	// flag is cleared by the call); synchronises the library stream
+	int TcStatus();
+	long long TcLaunches() const { return tc_launches_; }
 
 private:
 	int gpu_ready(int need) const { return (status_gpu_ & need) == need; }
@@ -218,6 +229,9 @@ private:
 	int* d_plas_ = nullptr;         // per-wave plasmon shifts of a scan chunk [nobj][nwave][2]
 	size_t plas_cap_ = 0;
 	long long launches_ = 0;
+	int prec_ = 0;                  // 0 FP32, 1 BF16 hi+lo tensor core, 2 FP16 hi+lo tensor core
+	int* d_tcerr_ = nullptr;        // tensor-core pass status word
+	long long tc_launches_ = 0;
 	cudaError_t last_cuda_ = cudaSuccess;
 };
 

@@ -91,6 +91,17 @@ int plan_count(int n);
 const PlanOps* plan_get(int n, int idx);
 inline bool pass_supported(int n) { return plan_count(n) > 0; }
 
+// Tensor-core forms of the row and column passes (jms_tc.cu) for line lengths
+// 256, 512 and 1024: prec 1 = BF16 hi+lo operands, 2 = FP16 hi+lo, FP32
+// accumulation.  No readout; the column pass needs a grating of the grid size
+// and no plasmon shift.  *err is set to 1 if a tensor-core wait ran out.
+bool tc_supported(int n);
+// builds the DFT-matrix tables of the tensor-core passes on the current device
+// (once per device, before the first pass; synchronises s)
+cudaError_t tc_prepare(cudaStream_t s);
+cudaError_t launch_tc_row(const PassArgs& p, int prec, int* err, cudaStream_t s);
+cudaError_t launch_tc_col(const PassArgs& p, int prec, int* err, cudaStream_t s);
+
 // det_int[w][plane][d] += weight * sum_blk partial[w][plane][d][blk] (FP64)
 cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
 	double* det_int, cudaStream_t s);

@@ -24,6 +24,7 @@
 #pragma once
 #include "jms_fft.cuh"
 #include "jms_kernels.h"
+#include "jms_launch.cuh"
 #include "jms_sizes.h"
 
 namespace jms {
@@ -856,12 +857,11 @@ cudaError_t launch_pipe(K kern, int threads, int smem, long long ntiles, cudaStr
 		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 		if (e != cudaSuccess) return e;
 	}
-	int dev = 0, nsm = 0, per_sm = 0;
+	int dev = 0, nsm = 0, per_sm = 1;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+	cudaError_t e = resident_ctas(kern, threads, smem, 32, &per_sm);
 	if (e != cudaSuccess) return e;
-	if (per_sm < 1) return cudaErrorInvalidConfiguration;
 	const long long g = (long long)nsm * per_sm;
 	kern<<<(unsigned)(ntiles < g ? ntiles : g), threads, smem, s>>>(args...);
 	return cudaGetLastError();
