@@ -34,6 +34,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "multislice steps/s (512² wave)"
 UNIT = "steps/s"
+# tensor-core forms reported beside the FP32 headline: (JMS_SetPrecision mode, name)
+TC_FORMS = ((1, "bf16"), (2, "fp16"))
+# tensor FLOPs per point of one 512-point pass: 4 radix stages (32, 16, 16, 32),
+# 5 hi/lo products of 8 R flops per point each
+TC_FLOP_PER_POINT = 5 * 8 * (32 + 16 + 16 + 32)
 
 
 def peaks():
@@ -294,6 +299,46 @@ def run_ours(args):
     J.L.JMS_PassTiming(C.byref(mc), C.byref(nc), C.byref(mr), C.byref(nr))
     J.L.JMS_SetPassTiming(0)
     barrier()
+    # tensor-core forms of the same step (JMS_SetPrecision), reported beside
+    # the FP32 headline: steps/s and per-pass device times
+    tc_forms = {}
+    if world == 1 and not args.no_tc:
+        N_ = cfg["nx"] * cfg["ny"]
+        for mode, form in TC_FORMS:
+            if J.set_precision(mode) != 0:
+                tc_forms[form] = {"value": None, "note": "JMS_SetPrecision failed"}
+                continue
+            tc0 = J.L.JMS_TcLaunches()
+            with torch.cuda.stream(stream):
+                step(0)
+            torch.cuda.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                t0.record(stream)
+                for k in range(2):
+                    step(1 + k)
+                t1.record(stream)
+            torch.cuda.synchronize()
+            ms_tc = t0.elapsed_time(t1) / 2
+            J.L.JMS_SetPassTiming(1)
+            with torch.cuda.stream(stream):
+                step(3)
+            torch.cuda.synchronize()
+            tmc, tmr = C.c_double(0), C.c_double(0)
+            tnc, tnr = C.c_longlong(0), C.c_longlong(0)
+            J.L.JMS_PassTiming(C.byref(tmc), C.byref(tnc), C.byref(tmr), C.byref(tnr))
+            J.L.JMS_SetPassTiming(0)
+            status = J.tc_status()
+            ntc = J.L.JMS_TcLaunches() - tc0
+            J.set_precision(0)
+            col_us = 1e3 * tmc.value / max(tnc.value, 1)
+            waves = min(args.batch, npos_step)
+            flops = waves * N_ * TC_FLOP_PER_POINT   # one column-pass launch, 5 products per radix stage
+            tc_forms[form] = {"value": steps_per_bench_step / (ms_tc / 1e3), "unit": UNIT, "ms_per_step": ms_tc,
+                              "col_pass_us": col_us, "row_pass_us": 1e3 * tmr.value / max(tnr.value, 1),
+                              "col_pass_tflops": flops / (col_us * 1e-6) / 1e12,
+                              "col_pass_hbm_frac": waves * 24 * N_ / (col_us * 1e-6) / 1e9 / peaks()[0],
+                              "tc_launches": int(ntc), "tc_status": int(status)}
     if world > 1:
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -370,6 +415,11 @@ def run_ours(args):
                         "d2h_bytes_per_step": int(h_int.numel() * 4 + h_bin.numel() * 4)},
                 "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
                 "grating_generation": gen}
+        if tc_forms:
+            line["tensor_core"] = {"forms": tc_forms,
+                                   "note": "same step with the tensor-core passes (JMS_SetPrecision 1 = BF16 hi+lo, "
+                                           "2 = FP16 hi+lo; readout slices keep the FP32 passes); "
+                                           "col_pass_tflops counts 5 MMA products per radix stage"}
         if world == 1 and not args.no_cpu:
             try:
                 gen["cpu_reference"] = reference_grating_cpu(cfg)
@@ -387,7 +437,8 @@ def run_ours(args):
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                         "sample": f"not run: {ex}"}
         if world == 1 and not args.no_err:
-            line["err_vs_fp64"] = error_vs_oracle(J, cfg, sp, probe, pro, dets, pos)
+            line["err_vs_fp64"] = error_vs_oracle(J, cfg, sp, probe, pro, dets, pos,
+                                                  tc_forms=() if args.no_tc else TC_FORMS)
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -807,11 +858,12 @@ def traffic_from_profiles(kind):
     return None
 
 
-def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
+def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos, tc_forms=()):
     """Relative error of the integrated detector signals of one probe position
     (one phonon pass, 200 slices) against the FP64 oracle, per detector (max
     over the 11 readout planes, relative to that detector's largest signal),
-    next to the error of the reference's own FP32 CPU path on the same input."""
+    next to the error of the reference's own FP32 CPU path on the same input
+    and of the tensor-core forms tc_forms ((JMS_SetPrecision mode, name), ...)."""
     try:
         from oracle import oracle as OR
     except Exception as ex:
@@ -834,6 +886,12 @@ def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
     def rel(x):
         return [float(v) for v in np.abs(x - ref_fp64).max(axis=0) / den]
 
+    tc_rel = {}
+    for mode, form in tc_forms:
+        J.set_precision(mode)
+        e, out_tc, _ = J.scan(p, 1, varseq=var[None, :])
+        J.set_precision(0)
+        tc_rel[form] = rel(out_tc[0]) if e == 0 else f"scan returned {e}"
     out_d = {"det_rel": rel(out[0]), "abs_vs_beam": float(np.abs(out[0] - ref_fp64).max()),
              "signal_max": [float(v) for v in np.abs(ref_fp64).max(axis=0)],
              "sample": "1 position x 1 phonon pass x 200 slices, 11 planes x 3 detectors; "
@@ -859,6 +917,8 @@ def error_vs_oracle(J, cfg, sp, probe, pro, dets, pos):
         out_d["reference_fp32_det_rel"] = rel(rd)
     except Exception as ex:
         out_d["reference_fp32_det_rel"] = f"not run: {ex}"
+    if tc_rel:
+        out_d["tensor_core_det_rel"] = tc_rel
     return out_d
 
 
@@ -871,6 +931,7 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-err", action="store_true")
+    ap.add_argument("--no-tc", action="store_true", help="skip the tensor-core forms beside the headline")
     ap.add_argument("--workload", default="scan", choices=["scan", "uneven", "cv", "qep"],
                     help="scan: the headline 512^2 scan; uneven: 12 specimens of uneven grid sizes; "
                          "cv: control-variate frozen-phonon averaging with the learned surrogate; "

@@ -98,6 +98,21 @@ struct Geo {
 	static constexpr int kSmem = oW + R1 * TWS * 8;
 	__device__ static int prow(int l, int n2) { return COL ? n2 * L + l : l * R2 + n2; }
 	__device__ static int qrow(int l, int k1) { return COL ? k1 * L + l : l * R1 + k1; }
+	// byte offset of row m in a layout with row-group stride SB, split into a
+	// part from the line l (runtime) and a part from the digit (compile-time
+	// in the unrolled loops): off(row(l, d)) = lbase(l) + dconst(d)
+	template <int SB, int D>
+	__device__ static int lbase(int l)
+	{
+		if (COL) return L >= 8 ? (l >> 3) * SB + (l & 7) * 16 : l * 16;   // l < L
+		return l * (D / 8) * SB;                                           // D = digits per line (8 | D)
+	}
+	template <int SB>
+	__device__ static constexpr int dconst(int d)
+	{
+		if (COL) return L >= 8 ? d * (L / 8) * SB : ((d * L) >> 3) * SB + ((d * L) & 7) * 16;
+		return (d >> 3) * SB + (d & 7) * 16;
+	}
 	__device__ static void pinv(int m, int& l, int& n2)
 	{
 		if (COL) { l = m % L; n2 = m / L; }
@@ -275,15 +290,15 @@ __device__ __forceinline__ void write_pq(const float2 (&v)[kVal], uint8_t* ahi, 
 	for (int j = 0; j < G::JP; j++) {
 		int l, n2;
 		G::pinv(threadIdx.x + kThr * j, l, n2);
-		const int cb = (n2 >> 2) * G::LQ + (n2 & 3) * 4;
+		uint8_t* bh = ahi + G::template lbase<G::SQ, G::R1>(l) + (n2 >> 2) * G::LQ + (n2 & 3) * 4;
+		uint8_t* bl = bh + (alo - ahi);
 		#pragma unroll
 		for (int k1 = 0; k1 < G::R1; k1++) {
-			const int mq = G::qrow(l, k1);
-			const int off = (mq >> 3) * G::SQ + (mq & 7) * 16 + cb;
+			const int off = G::template dconst<G::SQ>(k1);
 			uint32_t h, lo;
 			PR::split2(v[j * G::R1 + k1].x * s, v[j * G::R1 + k1].y * s, h, lo);
-			*reinterpret_cast<uint32_t*>(ahi + off) = h;
-			*reinterpret_cast<uint32_t*>(alo + off) = lo;
+			*reinterpret_cast<uint32_t*>(bh + off) = h;
+			*reinterpret_cast<uint32_t*>(bl + off) = lo;
 		}
 	}
 }
@@ -297,15 +312,15 @@ __device__ __forceinline__ void write_qp(const float2 (&v)[kVal], uint8_t* ahi, 
 	for (int j = 0; j < G::JQ; j++) {
 		int l, k1;
 		G::qinv(threadIdx.x + kThr * j, l, k1);
-		const int cb = (k1 >> 2) * G::LP + (k1 & 3) * 4;
+		uint8_t* bh = ahi + G::template lbase<G::SP, G::R2>(l) + (k1 >> 2) * G::LP + (k1 & 3) * 4;
+		uint8_t* bl = bh + (alo - ahi);
 		#pragma unroll
 		for (int n2 = 0; n2 < G::R2; n2++) {
-			const int mp = G::prow(l, n2);
-			const int off = (mp >> 3) * G::SP + (mp & 7) * 16 + cb;
+			const int off = G::template dconst<G::SP>(n2);
 			uint32_t h, lo;
 			PR::split2(v[j * G::R2 + n2].x * s, v[j * G::R2 + n2].y * s, h, lo);
-			*reinterpret_cast<uint32_t*>(ahi + off) = h;
-			*reinterpret_cast<uint32_t*>(alo + off) = lo;
+			*reinterpret_cast<uint32_t*>(bh + off) = h;
+			*reinterpret_cast<uint32_t*>(bl + off) = lo;
 		}
 	}
 }
