@@ -172,15 +172,17 @@ __device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const fl
 	#pragma unroll
 	for (int i = 0; i < A; i++) v[i] = sm[Tile::template s_fwd<A, B>(line, k1, 2 * i + h)];
 	dft_reg<A, 1, 0, INV>(v);
-	// radix-2 across the pair: Y[k] = E[k] + W_B^k O[k], Y[k + A] = E[k] - W_B^k O[k]
+	// radix-2 across the pair: Y[k] = E[k] + W_B^k O[k], Y[k + A] = E[k] - W_B^k O[k].
+	// The odd thread twiddles its own value before the exchange, so both
+	// threads finish with one sign-weighted add: u + o (h = 0), o - u (h = 1).
+	const float sgn = h ? -1.f : 1.f;
 	static_for<A>([&](auto K) {
 		constexpr int k = K.value;
+		const float2 u = h ? twiddle_ct<k, B, INV>(v[k]) : v[k];
 		float2 o;
-		o.x = __shfl_xor_sync(0xffffffffu, v[k].x, Tile::kPartner);
-		o.y = __shfl_xor_sync(0xffffffffu, v[k].y, Tile::kPartner);
-		const float2 e = h ? o : v[k];
-		const float2 t = twiddle_ct<k, B, INV>(h ? v[k] : o);
-		v[k] = h ? csub(e, t) : cadd(e, t);
+		o.x = __shfl_xor_sync(0xffffffffu, u.x, Tile::kPartner);
+		o.y = __shfl_xor_sync(0xffffffffu, u.y, Tile::kPartner);
+		v[k] = make_float2(fmaf(sgn, u.x, o.x), fmaf(sgn, u.y, o.y));
 	});
 	__syncthreads();
 }
@@ -194,13 +196,16 @@ __device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const fl
 	int line, j;
 	Tile::template role<B>(tid, line, j);
 	const int n1 = j >> 1, h = j & 1;
-	// radix-2 decimation in frequency over n2 = k + A h across the pair
+	// radix-2 decimation in frequency over n2 = k + A h across the pair:
+	// v + o (h = 0), W_B^k (o - v) (h = 1)
+	const float sgn = h ? -1.f : 1.f;
 	static_for<A>([&](auto K) {
 		constexpr int k = K.value;
 		float2 o;
 		o.x = __shfl_xor_sync(0xffffffffu, v[k].x, Tile::kPartner);
 		o.y = __shfl_xor_sync(0xffffffffu, v[k].y, Tile::kPartner);
-		v[k] = h ? twiddle_ct<k, B, INV>(csub(o, v[k])) : cadd(v[k], o);
+		const float2 d = make_float2(fmaf(sgn, v[k].x, o.x), fmaf(sgn, v[k].y, o.y));
+		v[k] = h ? twiddle_ct<k, B, INV>(d) : d;
 	});
 	dft_reg<A, 1, 0, INV>(v);   // output q2 = 2 m + h
 	#pragma unroll
@@ -552,11 +557,15 @@ k_col_pass(const PassArgs p)
 	for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
 	int c, j;
 	T::template role<PL::T>(tid, c, j);
+	// 32-bit offsets within a wave (nx * ny < 2^31): one base pointer per
+	// thread and a row stride, instead of a 64-bit product per element
+	const int stride = PL::B * nx;
 	if (c < nval && j < PL::T) {
+		const float2* src = W + j * nx + c;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) {
 			const int y = j + PL::B * m;
-			if (y <= p.in_k1 || y >= p.in_k2) v[m] = W[(long long)y * nx + c];
+			if (y <= p.in_k1 || y >= p.in_k2) v[m] = src[m * stride];
 		}
 	}
 	PL::template to_mid<true, T>(v, sm, p.twy, tid);
@@ -571,7 +580,7 @@ k_col_pass(const PassArgs p)
 				for (int e = 0; e < PL::EMID; e++) {
 					const int y = PL::mid(pos, e);
 					if (READ) readout_real(p, b, y, x, v[e]);
-					v[e] = cmul(v[e], __ldg(t + (long long)y * nx));
+					v[e] = cmul(v[e], __ldg(t + y * nx));
 				}
 			}
 			else { // sub-frame grating repeated periodically
@@ -601,10 +610,11 @@ k_col_pass(const PassArgs p)
 	PL::template from_mid<false, T>(v, sm, p.twy, tid);
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
+		float2* dst = W + j * nx + c;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) {
 			const int y = j + PL::B * m;
-			if (y <= p.out_k1 || y >= p.out_k2) W[(long long)y * nx + c] = v[m];
+			if (y <= p.out_k1 || y >= p.out_k2) dst[m * stride] = v[m];
 		}
 	}
 }
