@@ -338,12 +338,18 @@ __device__ __forceinline__ void tmem_ld_row(uint32_t taddr, float2* dst16, float
 			(__uint_as_float(r[2 * q + 1]) + __uint_as_float(c[2 * q + 1])) * inv);
 }
 
-// One radix stage over the current A operand: MMAs by thread 0, commit,
-// bounded wait, then every thread reads its J rows of D (R complex each).
-// Returns false (uniformly over the block) if the MMAs did not complete.
+// One radix stage over the current A operand, in three steps:
+//   stage_issue: make the A writes visible to the tensor core, then thread 0
+//                issues the MMAs and commits them to the mbarrier;
+//   stage_wait:  thread 0 waits for them (bounded); the block learns the
+//                outcome at a barrier whose ordering the tcgen05 fences extend
+//                to the TMEM reads; false (uniformly) if they did not finish;
+//   stage_read:  every thread reads its J rows of D (R complex each).
+// Between issue and wait a thread may do work that does not touch A or D
+// (the passes prefetch their next tile there).
 template <int R, int J, int LB, int SB, class PR>
-__device__ __forceinline__ bool stage(float2 (&v)[kVal], const uint8_t* ahi, const uint8_t* alo, const uint8_t* f,
-	uint32_t tmem, uint32_t mbar, uint32_t& phase, float inv)
+__device__ __forceinline__ void stage_issue(const uint8_t* ahi, const uint8_t* alo, const uint8_t* f, uint32_t tmem,
+	uint32_t mbar)
 {
 	fence_async_smem();
 	fence_before_sync();
@@ -372,8 +378,10 @@ __device__ __forceinline__ bool stage(float2 (&v)[kVal], const uint8_t* ahi, con
 		}
 		mma_commit(mbar);
 	}
-	// one thread waits for the MMAs (bounded); the block learns the outcome at
-	// the barrier, whose ordering the tcgen05 fences extend to the TMEM reads
+}
+
+__device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t& phase)
+{
 	bool ok = true;
 	if (threadIdx.x == 0) {
 		ok = mbar_wait(mbar, phase, kMaxWaitCycles);
@@ -382,12 +390,29 @@ __device__ __forceinline__ bool stage(float2 (&v)[kVal], const uint8_t* ahi, con
 	phase ^= 1u;
 	if (__syncthreads_or(!ok)) return false;
 	fence_after_sync();
-	const uint32_t lane = (uint32_t)((threadIdx.x >> 5) * 32) << 16;
+	return true;
+}
+
+__device__ __forceinline__ uint32_t lane_base() { return (uint32_t)((threadIdx.x >> 5) * 32) << 16; }
+
+template <int R, int J>
+__device__ __forceinline__ void stage_read(float2 (&v)[kVal], uint32_t tmem, float inv)
+{
 	#pragma unroll
 	for (int i = 0; i < J; i++) {
 		#pragma unroll
-		for (int h = 0; h < R / 16; h++) tmem_ld_row(tmem + lane + (uint32_t)(i * 2 * R + 32 * h), &v[i * R + 16 * h], inv);
+		for (int h = 0; h < R / 16; h++)
+			tmem_ld_row(tmem + lane_base() + (uint32_t)(i * 2 * R + 32 * h), &v[i * R + 16 * h], inv);
 	}
+}
+
+template <int R, int J, int LB, int SB, class PR>
+__device__ __forceinline__ bool stage(float2 (&v)[kVal], const uint8_t* ahi, const uint8_t* alo, const uint8_t* f,
+	uint32_t tmem, uint32_t mbar, uint32_t& phase, float inv)
+{
+	stage_issue<R, J, LB, SB, PR>(ahi, alo, f, tmem, mbar);
+	if (!stage_wait(mbar, phase)) return false;
+	stage_read<R, J>(v, tmem, inv);
 	return true;
 }
 
@@ -435,24 +460,56 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 	bool ok = true;
 	float2 v[kVal];
 	float inv = 1.f, s = 1.f;
-
-	for (long long tile = blockIdx.x; tile < tt.ntiles; tile += gridDim.x) {
-		const int b = (int)(tile / tt.per_wave);
-		const int ti = (int)(tile - (long long)b * tt.per_wave);
+	// tile t -> wave b and first row (row pass) / column (column pass)
+	auto decode = [&](long long t, int& b, int& first) {
+		b = (int)(t / tt.per_wave);
+		const int ti = (int)(t - (long long)b * tt.per_wave);
+		first = (COL ? ti : (ti < tt.split ? ti : ti + tt.skip)) * L;
+	};
+	// input of tile t into v: row pass, set P (x[R2 n1 + n2] of the rows);
+	// column pass, set Q (conj of X[k1 + R1 k2] of the columns).  Rows outside
+	// the band of live Fourier rows read as zero.
+	auto load_tile = [&](long long t) {
+		int b, first;
+		decode(t, b, first);
+		const float2* W = p.work + (long long)b * p.wstride;
 		if (!COL) {
-			// ---- row pass: FT_x -> x P -> IFT_x over rows row0 .. row0 + L - 1
-			const int row0 = (ti < tt.split ? ti : ti + tt.skip) * L;
-			float2* W = p.work + (long long)b * p.wstride;
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
 				G::pinv(tid + kThr * j, l, n2);
-				const int y = row0 + l;
+				const int y = first + l;
 				const bool live = y <= p.row_k1 || y >= p.row_k2;
 				const float2* src = W + (long long)y * N + n2;
 				#pragma unroll
 				for (int n1 = 0; n1 < R1; n1++) v[j * R1 + n1] = live ? src[R2 * n1] : make_float2(0.f, 0.f);
 			}
+		}
+		else {
+			const int nx = p.nx;
+			#pragma unroll
+			for (int j = 0; j < G::JQ; j++) {
+				int l, k1;
+				G::qinv(tid + kThr * j, l, k1);
+				const float2* src = W + first + k1 * nx + l;
+				#pragma unroll
+				for (int k2 = 0; k2 < R2; k2++) {
+					const int y = k1 + R1 * k2;
+					v[j * R2 + k2] = (y <= p.in_k1 || y >= p.in_k2) ? conjf2(src[R1 * k2 * nx]) : make_float2(0.f, 0.f);
+				}
+			}
+		}
+	};
+	if (blockIdx.x < tt.ntiles) load_tile(blockIdx.x);
+
+	for (long long tile = blockIdx.x; tile < tt.ntiles; tile += gridDim.x) {
+		int b, first;
+		decode(tile, b, first);
+		const long long next = tile + gridDim.x;
+		float2* W = p.work + (long long)b * p.wstride;
+		if (!COL) {
+			// ---- row pass: FT_x -> x P -> IFT_x over rows first .. first + L - 1
+			const int row0 = first;
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, s);
 			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
@@ -487,35 +544,32 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_qp<G, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
+			stage_issue<R1, G::JP, G::LP, G::SP, PR>(ahi, alo, f1, tmem, mbar);
+			// v is free until the next tile: its loads overlap this last stage
+			if (next < tt.ntiles) load_tile(next);
+			if (!(ok = stage_wait(mbar, phase))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
 				G::pinv(tid + kThr * j, l, n2);
 				const int y = row0 + l;
-				if (y <= p.row_k1 || y >= p.row_k2) {
-					float2* dst = W + (long long)y * N + n2;
-					#pragma unroll
-					for (int n1 = 0; n1 < R1; n1++) dst[R2 * n1] = conjf2(v[j * R1 + n1]);
+				const bool live = y <= p.row_k1 || y >= p.row_k2;
+				float2* dst = W + (long long)y * N + n2;
+				#pragma unroll
+				for (int h = 0; h < R1 / 16; h++) {
+					float2 d[16];
+					tmem_ld_row(tmem + lane_base() + (uint32_t)(j * 2 * R1 + 32 * h), d, inv);
+					if (live) {
+						#pragma unroll
+						for (int q = 0; q < 16; q++) dst[R2 * (16 * h + q)] = conjf2(d[q]);
+					}
 				}
 			}
 		}
 		else {
-			// ---- column pass: IFT_y -> x t -> FT_y over columns col0 .. col0 + L - 1
+			// ---- column pass: IFT_y -> x t -> FT_y over columns first .. first + L - 1
 			const int nx = p.nx;
-			const int col0 = ti * L;
-			float2* W = p.work + (long long)b * p.wstride + col0;
-			#pragma unroll
-			for (int j = 0; j < G::JQ; j++) {
-				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
-				const float2* src = W + k1 * nx + l;
-				#pragma unroll
-				for (int k2 = 0; k2 < R2; k2++) {
-					const int y = k1 + R1 * k2;
-					v[j * R2 + k2] = (y <= p.in_k1 || y >= p.in_k2) ? conjf2(src[R1 * k2 * nx]) : make_float2(0.f, 0.f);
-				}
-			}
+			const int col0 = first;
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, s);
 			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
@@ -551,7 +605,10 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_pq<G, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
+			stage_issue<R2, G::JQ, G::LQ, G::SQ, PR>(ahi, alo, f2, tmem, mbar);
+			// v is free until the next tile: its loads overlap this last stage
+			if (next < tt.ntiles) load_tile(next);
+			if (!(ok = stage_wait(mbar, phase))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
@@ -560,11 +617,17 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 				// recomputes these addresses instead of keeping the loads' ones
 				// live across the tile (register pressure)
 				const int sx = opaque(nx);
-				float2* dst = W + k1 * sx + l;
+				float2* dst = W + col0 + k1 * sx + l;
 				#pragma unroll
-				for (int k2 = 0; k2 < R2; k2++) {
-					const int y = k1 + R1 * k2;
-					if (y <= p.out_k1 || y >= p.out_k2) dst[R1 * k2 * sx] = v[j * R2 + k2];
+				for (int h = 0; h < R2 / 16; h++) {
+					float2 d[16];
+					tmem_ld_row(tmem + lane_base() + (uint32_t)(j * 2 * R2 + 32 * h), d, inv);
+					#pragma unroll
+					for (int q = 0; q < 16; q++) {
+						const int k2 = 16 * h + q;
+						const int y = k1 + R1 * k2;
+						if (y <= p.out_k1 || y >= p.out_k2) dst[R1 * k2 * sx] = d[q];
+					}
 				}
 			}
 		}
