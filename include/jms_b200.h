@@ -154,6 +154,30 @@ int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const i
 	float* d_out_bin, int bin);
 /* Probe positions processed together in one pass sequence (default 32). */
 int JMS_SetScanBatch(int nwave);
+/* Multi-fidelity frozen-phonon scan (no counterpart in the reference, which
+ * averages every configuration at full cost, src/JMultiSlice.cpp:4513-4677
+ * per pass).  Estimates the npass-configuration average of context ctx_full
+ * from ONE full pass (configuration 0 of varseq) and npass passes of context
+ * ctx_low, a coarser grid of the same specimen, probe, detectors and slices:
+ *   est = f(c0) - (g(c0) - mean_c g)       (control variate, coefficient 1)
+ * The estimate is unbiased.  Its error is that of f - g across the
+ * configurations; for detectors inside the coarse grid's band limit the
+ * phonon fluctuations of f and g agree closely (ratio 1.0000 +- 1e-4 and
+ * correlation^2 = 1 - 1e-7 measured for 512^2 against 256^2).  Detectors
+ * outside it get g = 0, so the estimate is the single full pass there.
+ * varseq: npass x nobjslc variant indices (required; both contexts use the same
+ * configurations).  Device form: d_pos [npos][2] nm and d_out_int double
+ * [npos][ndetslc][ndet] on the device (d_out_int overwritten).  The two
+ * contexts run concurrently on their own streams, and the call returns
+ * without waiting.  d_pos must be ready for both streams.  Host form: host
+ * buffers, returns after the copy back.  Returns 0, 1 (bad arguments or
+ * context), 2 (a context lacks its stream / setup), 3 (the contexts' slice or
+ * detector counts differ), 4 (scratch allocation), 5 (CUDA error), or an error
+ * of the scans. */
+int JMS_ScanMultiFidelityDevice(int ctx_full, int ctx_low, int npos, const float* d_pos, float dz, int npass,
+	const int* varseq, double* d_out_int);
+int JMS_ScanMultiFidelity(int ctx_full, int ctx_low, int npos, const float* pos, float dz, int npass,
+	const int* varseq, float* out_int);
 /* Kernel launches issued by the library so far. */
 long long JMS_KernelLaunches(void);
 /* Per-pass device timing: while on, each column and row pass launch is

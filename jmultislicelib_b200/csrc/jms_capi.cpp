@@ -6,6 +6,7 @@
 #include "jms_kernels.h"
 #include "jms_pgr_host.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -174,6 +175,84 @@ int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const i
 	float* d_out_bin, int bin)
 { return J().ScanGPUDevice(npos, d_pos, dz, npass, varseq, d_out_int, d_out_bin, bin); }
 int JMS_SetScanBatch(int nwave) { return J().SetScanBatch(nwave); }
+
+// Multi-fidelity frozen-phonon scan: the control-variate estimate
+//   est = f(c0) + (npass - 1) / npass * (mean_{c1..} g - g(c0))
+//       = f(c0) - (g(c0) - mean_{c0..} g)          (beta = 1)
+// of the npass-configuration average of the full-grid context, from one
+// full-grid pass (configuration c0) and npass passes of the coarse context.
+// Both contexts run on their own streams (concurrently); the full context's
+// stream waits for the coarse one before the combination.
+int JMS_ScanMultiFidelityDevice(int ctx_full, int ctx_low, int npos, const float* d_pos, float dz, int npass,
+	const int* varseq, double* d_out_int)
+{
+	JmsB200 *F = nullptr, *Lo = nullptr;
+	{
+		std::lock_guard<std::mutex> lock(g_ctx_mu);
+		F = ctx_get(ctx_full);
+		Lo = ctx_get(ctx_low);
+	}
+	if (F == nullptr || Lo == nullptr || F == Lo) return 1;
+	if (npos < 1 || npass < 1 || d_pos == nullptr || varseq == nullptr || d_out_int == nullptr) return 1;
+	const int nd = F->GetDetetionSliceNum(), ndet = F->GetDetNum(), nobj = F->GetObjectSliceNum();
+	if (nd != Lo->GetDetetionSliceNum() || ndet != Lo->GetDetNum() || nobj != Lo->GetObjectSliceNum() || nd < 1 ||
+		ndet < 1)
+		return 3;
+	if (F->Stream() == nullptr || Lo->Stream() == nullptr) return 2;
+	const size_t n = (size_t)npos * nd * ndet;
+	double* g = Lo->Scratch(2 * n);
+	if (g == nullptr) return 4;
+	double *g1 = g, *gm = g + n;
+	cudaStream_t sf = F->Stream(), sl = Lo->Stream();
+	if (cudaMemsetAsync(d_out_int, 0, sizeof(double) * n, sf) != cudaSuccess) return 5;
+	if (cudaMemsetAsync(g, 0, sizeof(double) * 2 * n, sl) != cudaSuccess) return 5;
+	int e = F->ScanGPUDevice(npos, d_pos, dz, 1, varseq, d_out_int, nullptr, 0);
+	if (e) return e;
+	e = Lo->ScanGPUDevice(npos, d_pos, dz, 1, varseq, g1, nullptr, 0);
+	if (e) return e;
+	if (npass > 1) {
+		e = Lo->ScanGPUDevice(npos, d_pos, dz, npass - 1, varseq + nobj, gm, nullptr, 0);
+		if (e) return e;
+		cudaEvent_t ev;
+		if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return 5;
+		cudaEventRecord(ev, sl);
+		cudaStreamWaitEvent(sf, ev, 0);
+		cudaEventDestroy(ev);
+		if (jms::launch_cv_combine(d_out_int, g1, gm, (long long)n, (double)(npass - 1) / (double)npass, sf) !=
+			cudaSuccess)
+			return 5;
+	}
+	return 0;
+}
+
+int JMS_ScanMultiFidelity(int ctx_full, int ctx_low, int npos, const float* pos, float dz, int npass,
+	const int* varseq, float* out_int)
+{
+	if (npos < 1 || pos == nullptr || out_int == nullptr) return 1;
+	JmsB200* F = nullptr;
+	{
+		std::lock_guard<std::mutex> lock(g_ctx_mu);
+		F = ctx_get(ctx_full);
+	}
+	if (F == nullptr || F->Stream() == nullptr) return 1;
+	const size_t n = (size_t)npos * std::max(1, F->GetDetetionSliceNum()) * std::max(1, F->GetDetNum());
+	// device copies of the positions and the estimate, in the full context's scratch
+	double* d = F->Scratch(n + (size_t)npos);
+	if (d == nullptr) return 4;
+	double* d_out = d;
+	float* d_pos = reinterpret_cast<float*>(d + n);
+	cudaStream_t sf = F->Stream();
+	if (cudaMemcpyAsync(d_pos, pos, sizeof(float) * 2 * (size_t)npos, cudaMemcpyHostToDevice, sf) != cudaSuccess)
+		return 5;
+	if (cudaStreamSynchronize(sf) != cudaSuccess) return 5;    // the coarse context reads d_pos on its own stream
+	int e = JMS_ScanMultiFidelityDevice(ctx_full, ctx_low, npos, d_pos, dz, npass, varseq, d_out);
+	if (e) return e;
+	std::vector<double> h(n);
+	if (cudaMemcpyAsync(h.data(), d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, sf) != cudaSuccess) return 5;
+	if (cudaStreamSynchronize(sf) != cudaSuccess) return 5;
+	for (size_t i = 0; i < n; i++) out_int[i] = (float)h[i];
+	return 0;
+}
 long long JMS_KernelLaunches(void) { return J().KernelLaunches(); }
 void JMS_SetPassTiming(int on) { J().SetPassTiming(on); }
 int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row)

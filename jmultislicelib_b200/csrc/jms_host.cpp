@@ -64,6 +64,7 @@ JmsB200::~JmsB200()
 	dfree(d_partial_);
 	dfree(d_shift_);
 	dfree(d_tcerr_);
+	dfree(d_scratch_);
 	if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1022,6 +1023,17 @@ int JmsB200::SetPrecision(int mode)
 	if (mode > 0 && post(tc_prepare(stream_), "tensor-core tables")) return 2;
 	prec_ = mode;
 	return 0;
+}
+
+double* JmsB200::Scratch(size_t n)
+{
+	if (n <= scratch_cap_ && d_scratch_) return d_scratch_;
+	if (stream_) cudaStreamSynchronize(stream_);   // the old buffer may still be in use
+	dfree(d_scratch_);
+	scratch_cap_ = 0;
+	if (post(cudaMalloc(&d_scratch_, sizeof(double) * n), "scratch")) return nullptr;
+	scratch_cap_ = n;
+	return d_scratch_;
 }
 
 int JmsB200::TcStatus()

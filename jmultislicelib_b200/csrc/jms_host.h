@@ -59,6 +59,7 @@ public:
 	void SetSliceThickness(int islc, float t);
 	float GetSliceThickness(int islc) const;
 	int GetDetetionSliceNum() const { return ndetslc_; }
+	int GetObjectSliceNum() const { return nobjslc_; }
 	int GetDetNum() const { return ndet_; }
 	int SetDetectionPlanes(int ndetper, int nobjslc, int* det_objslc) const;
 	int SetDetectionPlanesList(const int* slc_det, int nlist, int nobjslc, int* det_objslc) const;
@@ -162,6 +163,10 @@ public:
 	// flag is cleared by the call); synchronises the library stream
 	int TcStatus();
 	long long TcLaunches() const { return tc_launches_; }
+	// device scratch of at least n doubles, owned by the context (grown on
+	// demand, freed with it); nullptr if the allocation fails
+	double* Scratch(size_t n);
+	int Status() const { return status_gpu_; }
 
 private:
 	int gpu_ready(int need) const { return (status_gpu_ & need) == need; }
@@ -232,6 +237,8 @@ private:
 	int prec_ = 0;                  // 0 FP32, 1 BF16 hi+lo tensor core, 2 FP16 hi+lo tensor core
 	int* d_tcerr_ = nullptr;        // tensor-core pass status word
 	long long tc_launches_ = 0;
+	double* d_scratch_ = nullptr;
+	size_t scratch_cap_ = 0;
 	cudaError_t last_cuda_ = cudaSuccess;
 };
 

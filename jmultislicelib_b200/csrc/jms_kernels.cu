@@ -37,6 +37,20 @@ __global__ void k_abs2(float* __restrict__ out, const float2* __restrict__ in, l
 	out[i] = v.x * v.x + v.y * v.y;
 }
 
+__global__ void k_cv_combine(double* __restrict__ out, const double* __restrict__ g1, const double* __restrict__ gm,
+	long long n, double c)
+{
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] += c * (gm[i] - g1[i]);
+}
+
+cudaError_t launch_cv_combine(double* out, const double* g1, const double* gm, long long n, double c, cudaStream_t s)
+{
+	if (n <= 0) return cudaSuccess;
+	k_cv_combine<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, g1, gm, n, c);
+	return cudaGetLastError();
+}
+
 __global__ void k_finalize(const float* __restrict__ partial, int n, int nblk, float weight, double* det_int)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;

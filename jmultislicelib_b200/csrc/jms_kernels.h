@@ -119,6 +119,10 @@ int launch_readout_noalloc(const float2* wav, int nwave, int nx, int ny, const f
 	cudaStream_t s);
 int noalloc_capacity();
 
+// out[i] += c (gm[i] - g1[i]), i < n: the control-variate correction of the
+// multi-fidelity scan (JMS_ScanMultiFidelityDevice)
+cudaError_t launch_cv_combine(double* out, const double* g1, const double* gm, long long n, double c, cudaStream_t s);
+
 // out[i] = |in[i]|^2, i < n
 cudaError_t launch_abs2(float* out, const float2* in, long long n, cudaStream_t s);
 

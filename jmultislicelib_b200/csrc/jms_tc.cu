@@ -55,7 +55,9 @@ namespace jms {
 namespace tc {
 
 constexpr int kTile = 4096;           // complex points per tile
-constexpr int kThr = 128;             // threads per CTA = TMEM lanes = MMA M
+constexpr int kLanes = 128;           // rows of an MMA tile = TMEM lanes (M = 128)
+constexpr int kQ = 4;                 // threads per TMEM lane: each holds a quarter of its rows' values
+constexpr int kThr = kLanes * kQ;     // threads per CTA
 constexpr int kVal = kTile / kThr;    // complex values per thread
 constexpr int kDCols = 64;            // FP32 accumulator columns of a stage (2 T / 128)
 constexpr int kTmemCols = 2 * kDCols; // main products and correction products in separate accumulators
@@ -85,9 +87,11 @@ struct Geo {
 	static constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
 	static constexpr int L = kTile / N;                  // lines per tile
 	static constexpr int MP = L * R2, MQ = L * R1;       // rows of sets P and Q
-	static constexpr int JP = MP / kThr, JQ = MQ / kThr; // rows per thread
+	static constexpr int JP = MP / kLanes, JQ = MQ / kLanes; // rows per TMEM lane (and per thread)
+	static constexpr int VP = R1 / kQ, VQ = R2 / kQ;         // values per thread and row in P / Q
 	static constexpr int LP = Lay<N, COL>::lp, SP = Lay<N, COL>::sp, LQ = Lay<N, COL>::lq, SQ = Lay<N, COL>::sq;
-	static_assert(MP % kThr == 0 && MQ % kThr == 0, "tile rows must fill M = 128");
+	static_assert(MP % kLanes == 0 && MQ % kLanes == 0, "tile rows must fill M = 128");
+	static_assert(VP % 4 == 0 && VQ % 4 == 0, "a thread writes whole 16-byte chunks of its rows");
 	static_assert(SP >= (R1 / 4) * LP && SQ >= (R2 / 4) * LQ, "layout rows overlap");
 	static constexpr int bytes(int M, int KC, int lbo, int sbo) { return (M / 8 - 1) * sbo + (KC - 1) * lbo + 128; }
 	static constexpr int kA = rup(cmax(bytes(MP, R1 / 4, LP, SP), bytes(MQ, R2 / 4, LQ, SQ)), 1024);
@@ -250,7 +254,9 @@ __device__ __forceinline__ float tile_scale(const float2 (&v)[kVal], float* red,
 		for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 		if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
 		__syncthreads();
-		mx = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
+		mx = 0.f;
+		#pragma unroll
+		for (int w = 0; w < kThr / 32; w++) mx = fmaxf(mx, red[w]);
 		int e = 0;
 		if (mx > 0.f) frexpf(mx, &e);
 		e = max(min(e, 100), -100);
@@ -259,82 +265,96 @@ __device__ __forceinline__ float tile_scale(const float2 (&v)[kVal], float* red,
 	}
 }
 
-// A operand of a set whose rows are the thread's own rows (t + 128 j): row
-// m, 16-byte chunk c = values 4c .. 4c+3 (8 16-bit numbers)
+// Thread t serves TMEM lane t % 128 (rows t % 128 + 128 j of the current
+// set) and quarter q = t / 128 of those rows' values: value index q V + i,
+// i < V = R / 4, held in v[j V + i].
+__device__ __forceinline__ int lane_of() { return threadIdx.x & (kLanes - 1); }
+__device__ __forceinline__ int quarter_of() { return threadIdx.x >> 7; }
+
+// A operand of a set whose rows are the thread's own rows: row m, 16-byte
+// chunk c = values 4c .. 4c+3 (8 16-bit numbers); the thread writes the
+// chunks of its quarter
 template <int R, int J, int LB, int SB, class PR>
 __device__ __forceinline__ void write_own(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
 {
+	constexpr int V = R / kQ;
 	#pragma unroll
 	for (int j = 0; j < J; j++) {
-		const int m = threadIdx.x + kThr * j;
-		const int base = (m >> 3) * SB + (m & 7) * 16;
+		const int m = lane_of() + kLanes * j;
+		const int base = (m >> 3) * SB + (m & 7) * 16 + quarter_of() * (V / 4) * LB;
 		#pragma unroll
-		for (int c = 0; c < R / 4; c++) {
+		for (int c = 0; c < V / 4; c++) {
 			uint4 h, l;
-			PR::split2(v[j * R + 4 * c + 0].x * s, v[j * R + 4 * c + 0].y * s, h.x, l.x);
-			PR::split2(v[j * R + 4 * c + 1].x * s, v[j * R + 4 * c + 1].y * s, h.y, l.y);
-			PR::split2(v[j * R + 4 * c + 2].x * s, v[j * R + 4 * c + 2].y * s, h.z, l.z);
-			PR::split2(v[j * R + 4 * c + 3].x * s, v[j * R + 4 * c + 3].y * s, h.w, l.w);
+			PR::split2(v[j * V + 4 * c + 0].x * s, v[j * V + 4 * c + 0].y * s, h.x, l.x);
+			PR::split2(v[j * V + 4 * c + 1].x * s, v[j * V + 4 * c + 1].y * s, h.y, l.y);
+			PR::split2(v[j * V + 4 * c + 2].x * s, v[j * V + 4 * c + 2].y * s, h.z, l.z);
+			PR::split2(v[j * V + 4 * c + 3].x * s, v[j * V + 4 * c + 3].y * s, h.w, l.w);
 			*reinterpret_cast<uint4*>(ahi + base + c * LB) = h;
 			*reinterpret_cast<uint4*>(alo + base + c * LB) = l;
 		}
 	}
 }
 
-// transposing write P -> Q: the thread's P rows (l, n2) hold values over k1;
-// Q row (l, k1) gets value n2 at K position n2
+// transposing write P -> Q: the thread's P rows (l, n2) hold values over k1
+// (its quarter); Q row (l, k1) gets value n2 at K position n2
 template <class G, class PR>
 __device__ __forceinline__ void write_pq(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
 {
+	constexpr int V = G::VP;
 	#pragma unroll
 	for (int j = 0; j < G::JP; j++) {
 		int l, n2;
-		G::pinv(threadIdx.x + kThr * j, l, n2);
-		uint8_t* bh = ahi + G::template lbase<G::SQ, G::R1>(l) + (n2 >> 2) * G::LQ + (n2 & 3) * 4;
+		G::pinv(lane_of() + kLanes * j, l, n2);
+		uint8_t* bh = ahi + G::template lbase<G::SQ, G::R1>(l) + (n2 >> 2) * G::LQ + (n2 & 3) * 4 +
+			G::template dconst<G::SQ>(quarter_of() * V);
 		uint8_t* bl = bh + (alo - ahi);
 		#pragma unroll
-		for (int k1 = 0; k1 < G::R1; k1++) {
-			const int off = G::template dconst<G::SQ>(k1);
+		for (int i = 0; i < V; i++) {
+			const int off = G::template dconst<G::SQ>(i);   // k1 = q V + i
 			uint32_t h, lo;
-			PR::split2(v[j * G::R1 + k1].x * s, v[j * G::R1 + k1].y * s, h, lo);
+			PR::split2(v[j * V + i].x * s, v[j * V + i].y * s, h, lo);
 			*reinterpret_cast<uint32_t*>(bh + off) = h;
 			*reinterpret_cast<uint32_t*>(bl + off) = lo;
 		}
 	}
 }
 
-// transposing write Q -> P: the thread's Q rows (l, k1) hold values over n2;
-// P row (l, n2) gets value k1 at K position k1
+// transposing write Q -> P: the thread's Q rows (l, k1) hold values over n2
+// (its quarter); P row (l, n2) gets value k1 at K position k1
 template <class G, class PR>
 __device__ __forceinline__ void write_qp(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
 {
+	constexpr int V = G::VQ;
 	#pragma unroll
 	for (int j = 0; j < G::JQ; j++) {
 		int l, k1;
-		G::qinv(threadIdx.x + kThr * j, l, k1);
-		uint8_t* bh = ahi + G::template lbase<G::SP, G::R2>(l) + (k1 >> 2) * G::LP + (k1 & 3) * 4;
+		G::qinv(lane_of() + kLanes * j, l, k1);
+		uint8_t* bh = ahi + G::template lbase<G::SP, G::R2>(l) + (k1 >> 2) * G::LP + (k1 & 3) * 4 +
+			G::template dconst<G::SP>(quarter_of() * V);
 		uint8_t* bl = bh + (alo - ahi);
 		#pragma unroll
-		for (int n2 = 0; n2 < G::R2; n2++) {
-			const int off = G::template dconst<G::SP>(n2);
+		for (int i = 0; i < V; i++) {
+			const int off = G::template dconst<G::SP>(i);   // n2 = q V + i
 			uint32_t h, lo;
-			PR::split2(v[j * G::R2 + n2].x * s, v[j * G::R2 + n2].y * s, h, lo);
+			PR::split2(v[j * V + i].x * s, v[j * V + i].y * s, h, lo);
 			*reinterpret_cast<uint32_t*>(bh + off) = h;
 			*reinterpret_cast<uint32_t*>(bl + off) = lo;
 		}
 	}
 }
 
-// 16 complex values of a D row: main accumulator + correction accumulator
-__device__ __forceinline__ void tmem_ld_row(uint32_t taddr, float2* dst16, float inv)
+// V complex values (2V columns from taddr) of a D row: main accumulator +
+// correction accumulator
+template <int V>
+__device__ __forceinline__ void tmem_ld_vals(uint32_t taddr, float2* dst, float inv)
 {
-	uint32_t r[32], c[32];
-	tmem_ld32(taddr, r);
-	tmem_ld32(taddr + kDCols, c);
+	uint32_t r[2 * V], c[2 * V];
+	if constexpr (V == 4) { tmem_ld8(taddr, r); tmem_ld8(taddr + kDCols, c); }
+	else { tmem_ld16(taddr, r); tmem_ld16(taddr + kDCols, c); }
 	tmem_wait_ld();
 	#pragma unroll
-	for (int q = 0; q < 16; q++)
-		dst16[q] = make_float2((__uint_as_float(r[2 * q]) + __uint_as_float(c[2 * q])) * inv,
+	for (int q = 0; q < V; q++)
+		dst[q] = make_float2((__uint_as_float(r[2 * q]) + __uint_as_float(c[2 * q])) * inv,
 			(__uint_as_float(r[2 * q + 1]) + __uint_as_float(c[2 * q + 1])) * inv);
 }
 
@@ -356,7 +376,7 @@ __device__ __forceinline__ void stage_issue(const uint8_t* ahi, const uint8_t* a
 	__syncthreads();
 	if (threadIdx.x == 0) {
 		fence_after_sync();
-		constexpr uint32_t idesc = idesc_f16(PR::kFmt, kThr, 2 * R);
+		constexpr uint32_t idesc = idesc_f16(PR::kFmt, kLanes, 2 * R);
 		const uint32_t ah = smem_u32(ahi), al = smem_u32(alo), bh = smem_u32(f);
 		const uint32_t bm = bh + 8 * R * R, bl = bh + 16 * R * R;
 		#pragma unroll
@@ -393,17 +413,19 @@ __device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t& phase)
 	return true;
 }
 
-__device__ __forceinline__ uint32_t lane_base() { return (uint32_t)((threadIdx.x >> 5) * 32) << 16; }
+// TMEM address of the thread's lane quadrant (warp % 4) and quarter of a
+// stage's D row (tile i, radix R): lane bits 31..16, column bits 15..0
+template <int R>
+__device__ __forceinline__ uint32_t d_addr(uint32_t tmem, int i)
+{
+	return tmem + ((uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16) + (uint32_t)(i * 2 * R + quarter_of() * 2 * (R / kQ));
+}
 
 template <int R, int J>
 __device__ __forceinline__ void stage_read(float2 (&v)[kVal], uint32_t tmem, float inv)
 {
 	#pragma unroll
-	for (int i = 0; i < J; i++) {
-		#pragma unroll
-		for (int h = 0; h < R / 16; h++)
-			tmem_ld_row(tmem + lane_base() + (uint32_t)(i * 2 * R + 32 * h), &v[i * R + 16 * h], inv);
-	}
+	for (int i = 0; i < J; i++) tmem_ld_vals<R / kQ>(d_addr<R>(tmem, i), &v[i * (R / kQ)], inv);
 }
 
 template <int R, int J, int LB, int SB, class PR>
@@ -424,14 +446,14 @@ struct TcTiles {
 };
 
 template <int N, bool COL, class PR>
-__global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcTiles tt)
+__global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcTiles tt)
 {
 	using G = Geo<N, COL>;
-	constexpr int R1 = G::R1, R2 = G::R2, L = G::L;
+	constexpr int R1 = G::R1, R2 = G::R2, L = G::L, VP = G::VP, VQ = G::VQ;
 	extern __shared__ __align__(1024) uint8_t sm[];
 	__shared__ __align__(8) uint64_t mbar_s;
 	__shared__ uint32_t tbase_s;
-	__shared__ float red_s[4];
+	__shared__ float red_s[kThr / 32];
 	uint8_t* ahi = sm;
 	uint8_t* alo = sm + G::oAlo;
 	const uint8_t* f1 = sm + G::oF1;
@@ -441,6 +463,7 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 	float2* wt = reinterpret_cast<float2*>(sm + G::oW);
 	constexpr int TWS = G::TWS;
 	const int tid = threadIdx.x;
+	const int lane = lane_of(), q = quarter_of();
 	const float2* tw = COL ? p.twy : p.twx;
 
 	copy_dft<R1>(sm + G::oF1, PR::kFmt == 1 ? 0 : 1);
@@ -466,9 +489,10 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 		const int ti = (int)(t - (long long)b * tt.per_wave);
 		first = (COL ? ti : (ti < tt.split ? ti : ti + tt.skip)) * L;
 	};
-	// input of tile t into v: row pass, set P (x[R2 n1 + n2] of the rows);
-	// column pass, set Q (conj of X[k1 + R1 k2] of the columns).  Rows outside
-	// the band of live Fourier rows read as zero.
+	// input of tile t into v: row pass, set P (x[R2 n1 + n2] of the rows, n1 in
+	// the thread's quarter); column pass, set Q (conj of X[k1 + R1 k2] of the
+	// columns, k2 in the quarter).  Rows outside the band of live Fourier rows
+	// read as zero.
 	auto load_tile = [&](long long t) {
 		int b, first;
 		decode(t, b, first);
@@ -477,12 +501,12 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
-				G::pinv(tid + kThr * j, l, n2);
+				G::pinv(lane + kLanes * j, l, n2);
 				const int y = first + l;
 				const bool live = y <= p.row_k1 || y >= p.row_k2;
-				const float2* src = W + (long long)y * N + n2;
+				const float2* src = W + (long long)y * N + n2 + R2 * (q * VP);
 				#pragma unroll
-				for (int n1 = 0; n1 < R1; n1++) v[j * R1 + n1] = live ? src[R2 * n1] : make_float2(0.f, 0.f);
+				for (int i = 0; i < VP; i++) v[j * VP + i] = live ? src[R2 * i] : make_float2(0.f, 0.f);
 			}
 		}
 		else {
@@ -490,12 +514,13 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
-				const float2* src = W + first + k1 * nx + l;
+				G::qinv(lane + kLanes * j, l, k1);
+				const int k20 = q * VQ;
+				const float2* src = W + first + (k1 + R1 * k20) * nx + l;
 				#pragma unroll
-				for (int k2 = 0; k2 < R2; k2++) {
-					const int y = k1 + R1 * k2;
-					v[j * R2 + k2] = (y <= p.in_k1 || y >= p.in_k2) ? conjf2(src[R1 * k2 * nx]) : make_float2(0.f, 0.f);
+				for (int i = 0; i < VQ; i++) {
+					const int y = k1 + R1 * (k20 + i);
+					v[j * VQ + i] = (y <= p.in_k1 || y >= p.in_k2) ? conjf2(src[R1 * i * nx]) : make_float2(0.f, 0.f);
 				}
 			}
 		}
@@ -516,9 +541,9 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
-				G::pinv(tid + kThr * j, l, n2);
+				G::pinv(lane + kLanes * j, l, n2);
 				#pragma unroll
-				for (int k1 = 0; k1 < R1; k1++) v[j * R1 + k1] = cmul(v[j * R1 + k1], wt[k1 * TWS + n2]);
+				for (int i = 0; i < VP; i++) v[j * VP + i] = cmul(v[j * VP + i], wt[(q * VP + i) * TWS + n2]);
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_pq<G, PR>(v, ahi, alo, s);
@@ -527,10 +552,10 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
-				const float2* P = p.mul + (long long)(row0 + l) * N + k1;
+				G::qinv(lane + kLanes * j, l, k1);
+				const float2* P = p.mul + (long long)(row0 + l) * N + k1 + R1 * (q * VQ);
 				#pragma unroll
-				for (int k2 = 0; k2 < R2; k2++) v[j * R2 + k2] = conjf2(cmul(v[j * R2 + k2], __ldg(P + R1 * k2)));
+				for (int i = 0; i < VQ; i++) v[j * VQ + i] = conjf2(cmul(v[j * VQ + i], __ldg(P + R1 * i)));
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, s);
@@ -538,9 +563,9 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
+				G::qinv(lane + kLanes * j, l, k1);
 				#pragma unroll
-				for (int n2 = 0; n2 < R2; n2++) v[j * R2 + n2] = cmul(v[j * R2 + n2], wt[k1 * TWS + n2]);
+				for (int i = 0; i < VQ; i++) v[j * VQ + i] = cmul(v[j * VQ + i], wt[k1 * TWS + q * VQ + i]);
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_qp<G, PR>(v, ahi, alo, s);
@@ -551,18 +576,15 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
-				G::pinv(tid + kThr * j, l, n2);
+				G::pinv(lane + kLanes * j, l, n2);
 				const int y = row0 + l;
 				const bool live = y <= p.row_k1 || y >= p.row_k2;
-				float2* dst = W + (long long)y * N + n2;
-				#pragma unroll
-				for (int h = 0; h < R1 / 16; h++) {
-					float2 d[16];
-					tmem_ld_row(tmem + lane_base() + (uint32_t)(j * 2 * R1 + 32 * h), d, inv);
-					if (live) {
-						#pragma unroll
-						for (int q = 0; q < 16; q++) dst[R2 * (16 * h + q)] = conjf2(d[q]);
-					}
+				float2 d[VP];
+				tmem_ld_vals<VP>(d_addr<R1>(tmem, j), d, inv);
+				if (live) {
+					float2* dst = W + (long long)y * N + n2 + R2 * (q * VP);
+					#pragma unroll
+					for (int i = 0; i < VP; i++) dst[R2 * i] = conjf2(d[i]);
 				}
 			}
 		}
@@ -576,9 +598,9 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
+				G::qinv(lane + kLanes * j, l, k1);
 				#pragma unroll
-				for (int n2 = 0; n2 < R2; n2++) v[j * R2 + n2] = cmul(v[j * R2 + n2], wt[k1 * TWS + n2]);
+				for (int i = 0; i < VQ; i++) v[j * VQ + i] = cmul(v[j * VQ + i], wt[k1 * TWS + q * VQ + i]);
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_qp<G, PR>(v, ahi, alo, s);
@@ -587,11 +609,10 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
-				G::pinv(tid + kThr * j, l, n2);
-				const int sx = opaque(nx);
-				const float2* t = p.mul + col0 + l + n2 * sx;
+				G::pinv(lane + kLanes * j, l, n2);
+				const float2* t = p.mul + col0 + l + (n2 + R2 * (q * VP)) * nx;
 				#pragma unroll
-				for (int n1 = 0; n1 < R1; n1++) v[j * R1 + n1] = cmul(conjf2(v[j * R1 + n1]), __ldg(t + R2 * n1 * sx));
+				for (int i = 0; i < VP; i++) v[j * VP + i] = cmul(conjf2(v[j * VP + i]), __ldg(t + R2 * i * nx));
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, s);
@@ -599,9 +620,9 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
-				G::pinv(tid + kThr * j, l, n2);
+				G::pinv(lane + kLanes * j, l, n2);
 				#pragma unroll
-				for (int k1 = 0; k1 < R1; k1++) v[j * R1 + k1] = cmul(v[j * R1 + k1], wt[k1 * TWS + n2]);
+				for (int i = 0; i < VP; i++) v[j * VP + i] = cmul(v[j * VP + i], wt[(q * VP + i) * TWS + n2]);
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_pq<G, PR>(v, ahi, alo, s);
@@ -612,22 +633,15 @@ __global__ void __launch_bounds__(kThr, 3) k_tc_pass(const PassArgs p, const TcT
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
-				G::qinv(tid + kThr * j, l, k1);
-				// the row stride is re-read through an opaque move so the compiler
-				// recomputes these addresses instead of keeping the loads' ones
-				// live across the tile (register pressure)
-				const int sx = opaque(nx);
-				float2* dst = W + col0 + k1 * sx + l;
+				G::qinv(lane + kLanes * j, l, k1);
+				float2 d[VQ];
+				tmem_ld_vals<VQ>(d_addr<R2>(tmem, j), d, inv);
+				const int k20 = q * VQ;
+				float2* dst = W + col0 + (k1 + R1 * k20) * nx + l;
 				#pragma unroll
-				for (int h = 0; h < R2 / 16; h++) {
-					float2 d[16];
-					tmem_ld_row(tmem + lane_base() + (uint32_t)(j * 2 * R2 + 32 * h), d, inv);
-					#pragma unroll
-					for (int q = 0; q < 16; q++) {
-						const int k2 = 16 * h + q;
-						const int y = k1 + R1 * k2;
-						if (y <= p.out_k1 || y >= p.out_k2) dst[R1 * k2 * sx] = d[q];
-					}
+				for (int i = 0; i < VQ; i++) {
+					const int y = k1 + R1 * (k20 + i);
+					if (y <= p.out_k1 || y >= p.out_k2) dst[R1 * i * nx] = d[i];
 				}
 			}
 		}
