@@ -857,13 +857,31 @@ def run_qep(args):
     return 0
 
 
-def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=256):
+def coarse_grid(cfg, beta_mrad, lengths=(128, 160, 192, 240, 256, 320, 384)):
+    """Smallest supported grid length whose 2/3 band limit reaches beta_mrad
+    (same supercell): 2/3 * n / (2 a) * lambda >= beta."""
+    from jmultislicelib_b200 import synthetic as S
+
+    a = cfg["ncell"] * S.A_CELL                             # nm
+    v = cfg["kv"] * 1e3
+    lam = 1.2264262862 / np.sqrt(v * (1.0 + 9.7847538e-7 * v))   # relativistic electron wavelength, nm
+    for n in lengths:
+        if (2.0 / 3.0) * n / (2.0 * a) * lam * 1e3 >= beta_mrad:
+            return n
+    return cfg["nx"]
+
+
+def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=None):
     """The chosen form of the scan (JMS_ScanMultiFidelityDevice) against the plain
     one on the same raster rows and the same 16 phonon configurations: plain =
     16 full-grid passes per position; chosen = 1 full-grid pass + 16 passes on a
-    n_low^2 grid of the same specimen (control variate, coefficient 1).  Times
-    per raster row with CUDA events (inputs on the device) and the relative
-    difference of the estimate from the plain average, per detector."""
+    n_low^2 grid of the same specimen (control variate, coefficient 1), n_low
+    the coarsest supported grid whose band limit covers the 20-50 mrad detector
+    (192 at 300 kV on the 23.43 A cell: 54 mrad).  Times per raster row with
+    CUDA events (inputs on the device) and the relative difference of the
+    estimate from the plain average, per detector."""
+    if n_low is None:
+        n_low = coarse_grid(cfg, cfg["dets"][1][1])
     import ctypes as C
 
     import torch
