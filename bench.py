@@ -871,17 +871,21 @@ def coarse_grid(cfg, beta_mrad, lengths=(128, 160, 192, 240, 256, 320, 384)):
     return cfg["nx"]
 
 
-def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=None):
+def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=None, group=4):
     """The chosen form of the scan (JMS_ScanMultiFidelityDevice) against the plain
     one on the same raster rows and the same 16 phonon configurations: plain =
     16 full-grid passes per position; chosen = 1 full-grid pass + 16 passes on a
     n_low^2 grid of the same specimen (control variate, coefficient 1), n_low
     the coarsest supported grid whose band limit covers the 20-50 mrad detector
-    (192 at 300 kV on the 23.43 A cell: 54 mrad).  Times per raster row with
-    CUDA events (inputs on the device) and the relative difference of the
+    (192 at 300 kV on the 23.43 A cell: 54 mrad).  The chosen form takes
+    `group` raster rows per call, so that the coarse grid's launches carry
+    group x 64 waves (its 192^2 waves are small); the plain form takes one row
+    per call (64 waves of 512^2 already fill a launch).  Times per raster row
+    with CUDA events (inputs on the device) and the relative difference of the
     estimate from the plain average, per detector."""
     if n_low is None:
         n_low = coarse_grid(cfg, cfg["dets"][1][1])
+    rows = group * ((rows + group - 1) // group)
     import ctypes as C
 
     import torch
@@ -898,7 +902,7 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
         sp_lo = S.make_specimen(n_low, n_low, c_lo["ncell"], c_lo["ncell"], c_lo["nslice_types"], c_lo["nvar"],
                                 c_lo["seed"], c_lo["kv"])
         S.setup_library(J, c_lo, specimen=sp_lo)
-        J.L.JMS_SetScanBatch(64)
+        J.L.JMS_SetScanBatch(64 * group)
         J.L.JMS_SelectContext(0)
         nd, ndet = J.L.GetDetetionSliceNum(), J.L.GetDetNum()
         dev = d_pos.device
@@ -912,8 +916,12 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
                 raise RuntimeError(f"JMS_ScanGPUDevice returned {e}")
 
         def chosen(r):
-            p = d_pos[r * npos_step:(r + 1) * npos_step]
-            e = J.L.JMS_ScanMultiFidelityDevice(0, lo, npos_step, p.data_ptr(), 0.0, npass, vs, o_cv[r].data_ptr())
+            # rows r .. r + group - 1 in one call (r a multiple of group)
+            if r % group:
+                return
+            n = group * npos_step
+            p = d_pos[r * npos_step:r * npos_step + n]
+            e = J.L.JMS_ScanMultiFidelityDevice(0, lo, n, p.data_ptr(), 0.0, npass, vs, o_cv[r].data_ptr())
             if e:
                 raise RuntimeError(f"JMS_ScanMultiFidelityDevice returned {e}")
 
@@ -921,7 +929,7 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
         for name, fn in (("plain", plain), ("chosen", chosen)):
             with torch.cuda.stream(stream):
                 for k in range(warmup):
-                    fn(k % rows)
+                    fn((k * group) % rows)
             torch.cuda.synchronize()
             if name == "plain":
                 o_plain.zero_()        # the plain scan accumulates into its output
@@ -944,7 +952,8 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
                 "ms_per_row": res["chosen"], "plain_ms_per_row": res["plain"],
                 "speedup_vs_plain": res["plain"] / res["chosen"],
                 "scan_s": 64 * res["chosen"] / 1e3, "plain_scan_s": 64 * res["plain"] / 1e3,
-                "rows_timed": rows, "err_vs_plain_per_det": [float(x) for x in err],
+                "rows_timed": rows, "rows_per_chosen_call": group,
+                "err_vs_plain_per_det": [float(x) for x in err],
                 "note": "error relative to each detector's largest signal; the 80-200 mrad detector lies outside "
                         f"the {n_low}^2 band limit, so its estimate is the single full pass (its signal is 2e-10 "
                         "of the beam, below the FP32 noise of every form)"}
