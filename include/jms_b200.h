@@ -154,6 +154,16 @@ int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const i
 	float* d_out_bin, int bin);
 /* Probe positions processed together in one pass sequence (default 32). */
 int JMS_SetScanBatch(int nwave);
+/* Frozen-phonon configurations in one launch (no counterpart in the
+ * reference, whose GPUMultislice runs one wave per call,
+ * src/JMultiSlice.cpp:4513-4677).  When a scan has a variant sequence, more
+ * than one pass, fewer positions than the scan batch and no plasmon paths,
+ * several configurations of its positions share each launch sequence: each
+ * wave reads its own configuration's grating, and the detector sums and
+ * binned patterns of a position collect its waves in a fixed order.  on = 1
+ * (default) allows it, 0 runs one launch sequence per configuration.  Scans
+ * enqueued during a stream capture always take the sequential form. */
+int JMS_SetPassFusion(int on);
 /* Multi-fidelity frozen-phonon scan (no counterpart in the reference, which
  * averages every configuration at full cost, src/JMultiSlice.cpp:4513-4677
  * per pass).  Estimates the npass-configuration average of context ctx_full

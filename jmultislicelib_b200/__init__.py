@@ -75,7 +75,7 @@ SIGNATURES = {
     "JMS_SetStream": ([_p], _i),
     "JMS_ScanGPU": ([_i, _fp, _f, _i, _ip, _fp, _fp, _i], _i),
     "JMS_ScanGPUDevice": ([_i, _p, _f, _i, _ip, _p, _p, _i], _i),
-    "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong),
+    "JMS_SetScanBatch": ([_i], _i), "JMS_KernelLaunches": ([], C.c_longlong), "JMS_SetPassFusion": ([_i], _i),
     "JMS_ScanMultiFidelityDevice": ([_i, _i, _i, _p, _f, _i, _ip, _p], _i),
     "JMS_ScanMultiFidelity": ([_i, _i, _i, _fp, _f, _i, _ip, _fp], _i),
     "JMS_GridSupported": ([_i, _i], _i),

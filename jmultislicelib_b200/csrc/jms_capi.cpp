@@ -175,6 +175,7 @@ int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const i
 	float* d_out_bin, int bin)
 { return J().ScanGPUDevice(npos, d_pos, dz, npass, varseq, d_out_int, d_out_bin, bin); }
 int JMS_SetScanBatch(int nwave) { return J().SetScanBatch(nwave); }
+int JMS_SetPassFusion(int on) { return J().SetPassFusion(on); }
 
 // Multi-fidelity frozen-phonon scan: the control-variate estimate
 //   est = f(c0) + (npass - 1) / npass * (mean_{c1..} g - g(c0))

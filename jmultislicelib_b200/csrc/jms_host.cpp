@@ -65,6 +65,8 @@ JmsB200::~JmsB200()
 	dfree(d_shift_);
 	dfree(d_tcerr_);
 	dfree(d_scratch_);
+	dfree(d_mulw_);
+	dfree(d_shiftw_);
 	if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
 
@@ -617,7 +619,7 @@ int JmsB200::ensure_partial(int nwave)
 // of GPUMultislice (src/JMultiSlice.cpp:4611-4666).
 int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src,
 	const double* d_shift, int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx,
-	int nby, const int* plas, const int* d_plas_w)
+	int nby, const int* plas, const int* d_plas_w, const int* d_mulw, int wave_pos)
 {
 	if (!prow_ || !pcol_) return 2;
 	if (ensure_work(nwave) || ensure_partial(nwave)) return 1;
@@ -646,6 +648,7 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 	base.nbx = nbx;
 	base.nby = nby;
 	base.bin_plane = nobjslc_ >= 0 && !det_objslc_.empty() ? det_objslc_[nobjslc_] : -1;
+	base.wave_pos = wave_pos;
 	if (descan_on_) { base.descan_x = descan_x_; base.descan_y = descan_y_; }
 	PassArgs four = base, real = base;
 	if (single) {
@@ -676,7 +679,11 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		const int st = objslc_[j] % nscslc_;
 		const int ip = proidx_[st];
 		PassArgs c = real;
-		c.mul = d_pgr_ + slcoffset_[st] + (long long)var[j] * npgx_ * npgy_;
+		if (d_mulw) { // each wave its own configuration: offsets from the grating pool
+			c.mul = d_pgr_;
+			c.mul_w = d_mulw + (size_t)j * nwave;
+		}
+		else c.mul = d_pgr_ + slcoffset_[st] + (long long)var[j] * npgx_ * npgy_;
 		c.npgx = npgx_;
 		c.npgy = npgy_;
 		c.plane = b_img ? plane_of(j) : -1;
@@ -724,7 +731,8 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		launches_++;
 	}
 	if (base.ndet > 0) {
-		if (post(launch_finalize(d_partial_, nwave, ndetslc_, ndet_, base.nblk, weight, d_detint, s), "detector sums"))
+		if (post(launch_finalize(d_partial_, nwave, ndetslc_, ndet_, base.nblk, weight, d_detint, s, wave_pos),
+			"detector sums"))
 			return 701;
 		launches_++;
 	}
@@ -1094,6 +1102,60 @@ int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, co
 	const int B = std::max(1, scan_batch_);
 	std::vector<int> var((size_t)nobjslc_), plas_h;
 	const float w = 1.f / (float)npass;
+	// Fused configurations: with fewer positions than the batch, kp
+	// configurations of all positions share one launch sequence, wave
+	// k * npos + p being position p in configuration k.  Needs the variant
+	// sequence up front (no library draws), no plasmon paths, and grating
+	// offsets within int range.
+	const long long pool = slcoffset_.empty() ? 0
+		: slcoffset_.back() + (long long)nvarslc_.back() * npgx_ * npgy_;
+	// A stream capture keeps the sequential form: the fused form uploads its
+	// per-wave table from host memory on every call, which a graph could not
+	// replay.
+	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+	if (stream_) cudaStreamIsCapturing(stream_, &cap);
+	if (fuse_passes_ && varseq && npass > 1 && npos < B && !plasmon_on_ && pool < (1LL << 31) &&
+		cap == cudaStreamCaptureStatusNone) {
+		const int kp = std::min(npass, std::max(1, B / npos));
+		const size_t nw_max = (size_t)kp * npos;
+		if (nw_max * 4 > shiftw_cap_) {
+			dfree(d_shiftw_);
+			shiftw_cap_ = 0;
+			if (post(cudaMalloc(&d_shiftw_, sizeof(double) * 4 * nw_max), "ScanGPU")) return 1;
+			shiftw_cap_ = nw_max * 4;
+		}
+		if (nw_max * nobjslc_ > mulw_cap_) {
+			if (stream_) cudaStreamSynchronize(stream_);   // the old table may still be read
+			dfree(d_mulw_);
+			mulw_cap_ = 0;
+			if (post(cudaMalloc(&d_mulw_, sizeof(int) * nw_max * nobjslc_), "ScanGPU")) return 1;
+			mulw_cap_ = nw_max * nobjslc_;
+		}
+		for (int ip0 = 0; ip0 < npass; ip0 += kp) {
+			const int kk = std::min(kp, npass - ip0), nw = kk * npos;
+			h_mulw_.assign((size_t)nw * nobjslc_, 0);
+			for (int j = 0; j < nobjslc_; j++) {
+				const int st = objslc_[j] % nscslc_;
+				for (int k = 0; k < kk; k++) {
+					const int v = varseq[(size_t)(ip0 + k) * nobjslc_ + j];
+					const int off = (int)(slcoffset_[st] + (long long)v * npgx_ * npgy_);
+					for (int p = 0; p < npos; p++) h_mulw_[(size_t)j * nw + (size_t)k * npos + p] = off;
+				}
+			}
+			// stream order keeps the previous launch sequence's reads of the
+			// tables ahead of these writes
+			if (post(cudaMemcpyAsync(d_mulw_, h_mulw_.data(), sizeof(int) * h_mulw_.size(), cudaMemcpyHostToDevice,
+				stream_), "ScanGPU")) return 1;
+			if (post(launch_gather_shift(d_shiftw_, d_shift_, npos, nw, stream_), "ScanGPU")) return 1;
+			launches_++;
+			int e = run_slices(nw, 0, nullptr, w, d_wav0_, d_shiftw_, 0, 0, d_cppl_, d_out_int, d_out_bin, bin, nbx, nby,
+				nullptr, nullptr, d_mulw_, npos);
+			if (e) return e;
+			// the pageable host table is reused by the next group: its copy above
+			// has been staged already when cudaMemcpyAsync returned
+		}
+		return 0;
+	}
 	for (int p0 = 0; p0 < npos; p0 += B) {
 		const int nw = std::min(B, npos - p0);
 		for (int ip = 0; ip < npass; ip++) {

@@ -135,6 +135,10 @@ public:
 	// (jms_noalloc.cu); d_out is double [nwave][ndet], overwritten.
 	int ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, cudaStream_t s);
 	int SetScanBatch(int nwave) { scan_batch_ = nwave > 0 ? nwave : scan_batch_; return 0; }
+	// With a variant sequence and fewer positions than the scan batch, the scan
+	// puts several frozen-phonon configurations of the positions into one
+	// launch (on by default); off = one launch sequence per configuration.
+	int SetPassFusion(int on) { fuse_passes_ = on ? 1 : 0; return 0; }
 	// Line-plan choice (jms_sizes.h): Autotune times every candidate plan of
 	// nx (row passes) and ny (column passes) on nwave waves of the current
 	// setup and keeps the fastest; the choice is remembered per length for
@@ -173,9 +177,12 @@ private:
 	int post(cudaError_t e, const char* where);
 	int ensure_work(int nwave);
 	int ensure_partial(int nwave);
+	// d_mulw (with var == nullptr): per-slice per-wave grating offsets
+	// [nobjslc][nwave] of waves from several phonon configurations; wave_pos > 0:
+	// wave b is position b % wave_pos for the detector sums and binned patterns
 	int run_slices(int nwave, int islc0, const int* var, float weight, const float2* entry_src, const double* d_shift,
 		int ibtx, int ibty, const float* d_cppl, double* d_detint, float* d_bin, int bin, int nbx, int nby,
-		const int* plas = nullptr, const int* d_plas_w = nullptr);
+		const int* plas = nullptr, const int* d_plas_w = nullptr, const int* d_mulw = nullptr, int wave_pos = 0);
 	// one slice of the plasmon Monte-Carlo (CJPlasmonMC::ScatGridMC); returns
 	// the number of new excitations, (di, dj) the change of the pixel shift
 	int plasmon_step(float dt, int* di, int* dj);
@@ -239,6 +246,12 @@ private:
 	long long tc_launches_ = 0;
 	double* d_scratch_ = nullptr;
 	size_t scratch_cap_ = 0;
+	int fuse_passes_ = 1;
+	int* d_mulw_ = nullptr;         // per-slice per-wave grating offsets of a fused scan launch
+	size_t mulw_cap_ = 0;
+	double* d_shiftw_ = nullptr;    // per-wave probe offsets of a fused scan launch
+	size_t shiftw_cap_ = 0;
+	std::vector<int> h_mulw_;
 	cudaError_t last_cuda_ = cudaSuccess;
 };
 

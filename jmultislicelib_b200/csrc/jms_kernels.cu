@@ -51,14 +51,35 @@ cudaError_t launch_cv_combine(double* out, const double* g1, const double* gm, l
 	return cudaGetLastError();
 }
 
-__global__ void k_finalize(const float* __restrict__ partial, int n, int nblk, float weight, double* det_int)
+// thread i = (position p, plane, detector) of n outputs; m = ndetslc * ndet
+// elements per wave; the waves of position p are p + k * step, k < nk
+__global__ void k_finalize(const float* __restrict__ partial, int n, int m, int nblk, int step, int nk, float weight,
+	double* det_int)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	const float* src = partial + (long long)i * nblk;
+	const int pos = i / m, e = i - pos * m;
 	double s = 0.0;
-	for (int k = 0; k < nblk; k++) s += (double)src[k];
+	for (int k = 0; k < nk; k++) {
+		const float* src = partial + ((long long)(pos + k * step) * m + e) * nblk;
+		for (int b = 0; b < nblk; b++) s += (double)src[b];
+	}
 	det_int[i] += (double)weight * s;
+}
+
+__global__ void k_gather_shift(double* __restrict__ sh_w, const double* __restrict__ sh, int npos, int nwave)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= 4 * nwave) return;
+	const int w = i >> 2, c = i & 3;
+	sh_w[i] = sh[4 * (w % npos) + c];
+}
+
+cudaError_t launch_gather_shift(double* sh_w, const double* sh, int npos, int nwave, cudaStream_t s)
+{
+	if (nwave <= 0 || npos <= 0) return cudaSuccess;
+	k_gather_shift<<<(4 * nwave + 255) / 256, 256, 0, s>>>(sh_w, sh, npos, nwave);
+	return cudaGetLastError();
 }
 
 __global__ void k_offset(float2* out, const float2* __restrict__ wav0, int nx, int ny, double s0, double s1,
@@ -101,11 +122,14 @@ const PlanOps* plan_get(int n, int idx)
 }
 
 cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
-	double* det_int, cudaStream_t s)
+	double* det_int, cudaStream_t s, int wave_pos)
 {
-	const int n = nwave * ndetslc * ndet;
+	const int m = ndetslc * ndet;
+	const int npos = wave_pos > 0 ? wave_pos : nwave;
+	const int nk = wave_pos > 0 ? nwave / wave_pos : 1;
+	const int n = npos * m;
 	if (n <= 0) return cudaSuccess;
-	k_finalize<<<(n + 255) / 256, 256, 0, s>>>(partial, n, nblk, weight, det_int);
+	k_finalize<<<(n + 255) / 256, 256, 0, s>>>(partial, n, m, nblk, npos, nk, weight, det_int);
 	return cudaGetLastError();
 }
 

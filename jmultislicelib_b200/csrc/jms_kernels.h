@@ -57,6 +57,13 @@ struct PassArgs {
 	// real-space ramp exp(2 pi i (plas_x x / nx + plas_y y / ny)) with x t
 	int plas_x = 0, plas_y = 0;
 	const int* plas_w = nullptr;    // [nwave][2] per-wave shifts of this slice (replaces plas_x / plas_y)
+	// column pass: per-wave element offsets of each wave's grating from mul
+	// (waves of different frozen-phonon configurations in one launch);
+	// nullptr = the grating at mul for every wave
+	const int* mul_w = nullptr;
+	// > 0: wave b is probe position b % wave_pos (several configurations of
+	// the positions in one launch): binned patterns go to the position
+	int wave_pos = 0;
 	int store = 1;                  // row pass: 0 = stop after the readout (last slice)
 	// Band of live Fourier rows: row ky (scrambled index) can be nonzero only
 	// if ky <= k1 or ky >= k2.  Propagators vanish outside their band limit,
@@ -102,9 +109,15 @@ cudaError_t tc_prepare(cudaStream_t s);
 cudaError_t launch_tc_row(const PassArgs& p, int prec, int* err, cudaStream_t s);
 cudaError_t launch_tc_col(const PassArgs& p, int prec, int* err, cudaStream_t s);
 
-// det_int[w][plane][d] += weight * sum_blk partial[w][plane][d][blk] (FP64)
+// det_int[w][plane][d] += weight * sum_blk partial[w][plane][d][blk] (FP64);
+// with wave_pos > 0 the waves w = p + k wave_pos (k = 0, 1, ...) are summed
+// into position p, in that order (deterministic)
 cudaError_t launch_finalize(const float* partial, int nwave, int ndetslc, int ndet, int nblk, float weight,
-	double* det_int, cudaStream_t s);
+	double* det_int, cudaStream_t s, int wave_pos = 0);
+
+// sh_w[w] = sh[w % npos] (4 doubles each), w < nwave: per-wave probe offsets
+// of several configurations of the same positions
+cudaError_t launch_gather_shift(double* sh_w, const double* sh, int npos, int nwave, cudaStream_t s);
 
 // shift[i] = (dx/a, dy/b, fz/a^2, fz/b^2) from pos[i] = (dx, dy) [nm]
 cudaError_t launch_make_shift(double* d_shift, const float* d_pos, int npos, double a, double b, double fz,

@@ -392,8 +392,9 @@ __device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y,
 		int ux = kx + (p.nx >> 1); if (ux >= p.nx) ux -= p.nx;
 		int uy = y + (p.ny >> 1); if (uy >= p.ny) uy -= p.ny;
 		int bx = ux / p.bin, by = uy / p.bin;
+		const int bp = p.wave_pos > 0 ? b % p.wave_pos : b;   // the wave's probe position
 		if (bx < p.nbx && by < p.nby)
-			atomicAdd(p.bin_out + ((long long)b * p.nby + by) * p.nbx + bx, p.weight * pw);
+			atomicAdd(p.bin_out + ((long long)bp * p.nby + by) * p.nbx + bx, p.weight * pw);
 	}
 }
 
@@ -574,8 +575,9 @@ k_col_pass(const PassArgs p)
 		T::template role<PL::TMID>(tid, c, pos);
 		if (c < nval && pos < PL::TMID) {
 			const int x = col0 + c;
+			const float2* mul = p.mul + (p.mul_w ? __ldg(p.mul_w + b) : 0);   // this wave's grating
 			if (p.npgx == nx && p.npgy == p.ny) { // grating of the grid size
-				const float2* t = p.mul + x;
+				const float2* t = mul + x;
 				#pragma unroll
 				for (int e = 0; e < PL::EMID; e++) {
 					const int y = PL::mid(pos, e);
@@ -589,7 +591,7 @@ k_col_pass(const PassArgs p)
 				for (int e = 0; e < PL::EMID; e++) {
 					const int y = PL::mid(pos, e);
 					if (READ) readout_real(p, b, y, x, v[e]);
-					v[e] = cmul(v[e], __ldg(p.mul + (long long)(y % p.npgy) * p.npgx + xs));
+					v[e] = cmul(v[e], __ldg(mul + (long long)(y % p.npgy) * p.npgx + xs));
 				}
 			}
 			int sx = p.plas_x, sy = p.plas_y;
@@ -804,8 +806,9 @@ k_col_pass_pipe(const PassArgs p, int ncb, int ntiles)
 			T::template role<PL::TMID>(tid, c, pos);
 			if (c < nval && pos < PL::TMID) {
 				const int x = col0 + c;
+				const float2* mul = p.mul + (p.mul_w ? __ldg(p.mul_w + b) : 0);   // this wave's grating
 				if (p.npgx == nx && p.npgy == p.ny) {
-					const float2* tg = p.mul + x;
+					const float2* tg = mul + x;
 					#pragma unroll
 					for (int e = 0; e < PL::EMID; e++) v[e] = cmul(v[e], __ldg(tg + (long long)PL::mid(pos, e) * nx));
 				}
@@ -813,7 +816,7 @@ k_col_pass_pipe(const PassArgs p, int ncb, int ntiles)
 					const int xs = x % p.npgx;
 					#pragma unroll
 					for (int e = 0; e < PL::EMID; e++)
-						v[e] = cmul(v[e], __ldg(p.mul + (long long)(PL::mid(pos, e) % p.npgy) * p.npgx + xs));
+						v[e] = cmul(v[e], __ldg(mul + (long long)(PL::mid(pos, e) % p.npgy) * p.npgx + xs));
 				}
 				int sx = p.plas_x, sy = p.plas_y;
 				if (p.plas_w) { sx = __ldg(p.plas_w + 2 * b); sy = __ldg(p.plas_w + 2 * b + 1); }

@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
 				G::pinv(lane + kLanes * j, l, n2);
-				const float2* t = p.mul + col0 + l + (n2 + R2 * (q * VP)) * nx;
+				const float2* t = p.mul + (p.mul_w ? __ldg(p.mul_w + b) : 0) + col0 + l + (n2 + R2 * (q * VP)) * nx;
 				#pragma unroll
 				for (int i = 0; i < VP; i++) v[j * VP + i] = cmul(conjf2(v[j * VP + i]), __ldg(t + R2 * i * nx));
 			}
