@@ -234,6 +234,10 @@ def run_ours(args):
     bin_ = cfg["bin"]
     nbx, nby = cfg["nx"] // bin_, cfg["ny"] // bin_
     steps_per_bench_step = npos_step * npass * cfg["nobj"]
+    # waves per launch: with a batch larger than the row, the library puts
+    # batch // 64 phonon configurations of the row's positions into each launch
+    kp = min(npass, max(1, args.batch // npos_step)) if args.batch > npos_step else 1
+    waves = kp * npos_step if args.batch > npos_step else min(args.batch, npos_step)
     dev = torch.device("cuda", local)
     d_pos = torch.from_numpy(pos).to(dev)
     d_int = torch.zeros((len(pos), nd, ndet), dtype=torch.float64, device=dev)
@@ -250,7 +254,7 @@ def run_ours(args):
     import ctypes as C
     ms_r, ms_c = C.c_float(0), C.c_float(0)
     ir, ic = C.c_int(0), C.c_int(0)
-    if J.L.JMS_Autotune(min(args.batch, npos_step), 20, C.byref(ms_r), C.byref(ms_c), C.byref(ir), C.byref(ic)):
+    if J.L.JMS_Autotune(waves, 20, C.byref(ms_r), C.byref(ms_c), C.byref(ir), C.byref(ic)):
         raise RuntimeError("autotune failed")
     print(f"# library kernel launches before the warm-up: {J.L.JMS_KernelLaunches()}", file=sys.stderr)
     names = []
@@ -332,7 +336,6 @@ def run_ours(args):
             ntc = J.L.JMS_TcLaunches() - tc0
             J.set_precision(0)
             col_us = 1e3 * tmc.value / max(tnc.value, 1)
-            waves = min(args.batch, npos_step)
             flops = waves * N_ * TC_FLOP_PER_POINT   # one column-pass launch, 5 products per radix stage
             tc_forms[form] = {"value": steps_per_bench_step / (ms_tc / 1e3), "unit": UNIT, "ms_per_step": ms_tc,
                               "col_pass_us": col_us, "row_pass_us": 1e3 * tmr.value / max(tnr.value, 1),
@@ -395,7 +398,6 @@ def run_ours(args):
         hbm, src = peaks()
         # dominant pass: algorithmic bytes per launch = waves x 24 N (8N wave
         # read + 8N wave write + 8N grating or propagator read)
-        waves = min(args.batch, npos_step)
         kind, t_ms, n = ("row", mr.value, nr.value) if mr.value >= mc.value else ("column", mc.value, nc.value)
         plan = names[0] if kind == "row" else names[1]
         avg_s = (t_ms / max(n, 1)) / 1e3
@@ -403,7 +405,7 @@ def run_ours(args):
         achieved = algo / avg_s / 1e9
         roof = {"bound": "hbm", "kernel": f"k_{kind[:3]}_pass plan {plan} ({waves} waves)", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": f"{src} hbm_gbs",
-                "traffic": traffic_from_profiles(kind), "bytes_per_launch": algo,
+                "traffic": traffic_from_profiles(kind, waves), "bytes_per_launch": algo,
                 "avg_launch_us": avg_s * 1e6, "col_pass_us": 1e3 * mc.value / max(nc.value, 1),
                 "row_pass_us": 1e3 * mr.value / max(nr.value, 1)}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -413,7 +415,7 @@ def run_ours(args):
                                        "512x512 complex64, 3 annular detectors every 20 slices + 128x128 binned "
                                        "exit diffraction",
                            "grid": 512, "slices": cfg["nobj"], "positions_per_step": npos_step, "passes": npass,
-                           "batch_waves": args.batch, "parallelism": f"probe positions sharded over {world} GPU(s)",
+                           "batch_waves": waves, "configurations_per_launch": kp, "parallelism": f"probe positions sharded over {world} GPU(s)",
                            "fft_plans": {"row": names[0], "column": names[1], "tuned_row_us": 1e3 * ms_r.value,
                                          "tuned_col_us": 1e3 * ms_c.value},
                            "l2": f"inputs larger than L2 (128 MiB grating pool, {2 * waves} MiB of waves per "
@@ -851,7 +853,7 @@ def run_qep(args):
             "config": {"workload": "STEM scan row: 64 positions x 16 phonon passes x 200 slices, 512x512; every "
                                    "pass a new QEP configuration: 200 gratings generated on the device "
                                    "(sigma 0.08 A, Gaussian form factors, 2/3 band limit)",
-                       "batch_waves": args.batch},
+                       "batch_waves": min(args.batch, 64)},
             "grating_generation_share": gen_ms / ms, "clocks": clk.summary()}
     print(json.dumps(line))
     return 0
@@ -902,7 +904,7 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
         sp_lo = S.make_specimen(n_low, n_low, c_lo["ncell"], c_lo["ncell"], c_lo["nslice_types"], c_lo["nvar"],
                                 c_lo["seed"], c_lo["kv"])
         S.setup_library(J, c_lo, specimen=sp_lo)
-        J.L.JMS_SetScanBatch(64 * group)
+        J.L.JMS_SetScanBatch(1024)          # 4 configurations x 256 positions per coarse launch
         J.L.JMS_SelectContext(0)
         nd, ndet = J.L.GetDetetionSliceNum(), J.L.GetDetNum()
         dev = d_pos.device
@@ -962,12 +964,13 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
         J.L.JMS_DestroyContext(lo)
 
 
-def traffic_from_profiles(kind):
-    """DRAM bytes per launch of the pass, from the committed ncu summary."""
+def traffic_from_profiles(kind, waves):
+    """DRAM bytes per launch of the pass with `waves` waves, from the committed
+    ncu summary (line "traffic_bytes_per_launch_<waves>_waves: <bytes>")."""
     p = os.path.join(ROOT, "profiles", f"{kind}_pass_512.md")
     try:
         for line in open(p):
-            if line.startswith("traffic_bytes_per_launch_scaled:"):
+            if line.startswith(f"traffic_bytes_per_launch_{waves}_waves:"):
                 return float(line.split(":")[1])
     except Exception:
         pass
@@ -1044,7 +1047,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=1024,
+                    help="waves per launch; above the 64 positions of a row, 16 phonon configurations share a launch")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-err", action="store_true")
     ap.add_argument("--no-tc", action="store_true", help="skip the tensor-core forms beside the headline")

@@ -156,9 +156,10 @@ int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const i
 int JMS_SetScanBatch(int nwave);
 /* Frozen-phonon configurations in one launch (no counterpart in the
  * reference, whose GPUMultislice runs one wave per call,
- * src/JMultiSlice.cpp:4513-4677).  When a scan has a variant sequence, more
- * than one pass, fewer positions than the scan batch and no plasmon paths,
- * several configurations of its positions share each launch sequence: each
+ * src/JMultiSlice.cpp:4513-4677).  When a scan has more than one pass, fewer
+ * positions than the scan batch and no plasmon paths, several configurations
+ * of its positions share each launch sequence (without a variant sequence the
+ * library draws all configurations first, in the sequential order): each
  * wave reads its own configuration's grating, and the detector sums and
  * binned patterns of a position collect its waves in a fixed order.  on = 1
  * (default) allows it, 0 runs one launch sequence per configuration.  Scans

@@ -1104,9 +1104,8 @@ int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, co
 	const float w = 1.f / (float)npass;
 	// Fused configurations: with fewer positions than the batch, kp
 	// configurations of all positions share one launch sequence, wave
-	// k * npos + p being position p in configuration k.  Needs the variant
-	// sequence up front (no library draws), no plasmon paths, and grating
-	// offsets within int range.
+	// k * npos + p being position p in configuration k.  Needs no plasmon
+	// paths and grating offsets within int range.
 	const long long pool = slcoffset_.empty() ? 0
 		: slcoffset_.back() + (long long)nvarslc_.back() * npgx_ * npgy_;
 	// A stream capture keeps the sequential form: the fused form uploads its
@@ -1114,8 +1113,16 @@ int JmsB200::ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, co
 	// replay.
 	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
 	if (stream_) cudaStreamIsCapturing(stream_, &cap);
-	if (fuse_passes_ && varseq && npass > 1 && npos < B && !plasmon_on_ && pool < (1LL << 31) &&
+	if (fuse_passes_ && npass > 1 && npos < B && !plasmon_on_ && pool < (1LL << 31) &&
 		cap == cudaStreamCaptureStatusNone) {
+		// without a given sequence, draw every configuration now, in the order
+		// the sequential form would (one draw per pass, positions in one batch)
+		std::vector<int> drawn;
+		if (!varseq) {
+			drawn.resize((size_t)npass * nobjslc_);
+			for (int ip = 0; ip < npass; ip++) GetRandomVariantSequence(drawn.data() + (size_t)ip * nobjslc_);
+			varseq = drawn.data();
+		}
 		const int kp = std::min(npass, std::max(1, B / npos));
 		const size_t nw_max = (size_t)kp * npos;
 		if (nw_max * 4 > shiftw_cap_) {
