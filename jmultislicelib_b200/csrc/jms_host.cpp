@@ -67,6 +67,7 @@ JmsB200::~JmsB200()
 	dfree(d_scratch_);
 	dfree(d_mulw_);
 	dfree(d_shiftw_);
+	dfree(d_io_);
 	if (own_stream_ && stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1218,17 +1219,26 @@ int JmsB200::ScanGPU(int npos, const float* pos, float dz, int npass, const int*
 	float* out_bin, int bin)
 {
 	if (npos <= 0 || pos == nullptr) return 1;
-	float* d_pos = nullptr;
-	double* d_int = nullptr;
-	float* d_bin = nullptr;
 	const size_t nint = (size_t)npos * ndetslc_ * ndet_;
 	const size_t nb = out_bin && bin > 0 ? (size_t)npos * (nx_ / bin) * (ny_ / bin) : 0;
 	int e = 0;
 	cudaStream_t s = stream_;
-	if (post(cudaMallocAsync(&d_pos, sizeof(float) * 2 * npos, s), "ScanGPU")) return 1;
-	if (nint && post(cudaMallocAsync(&d_int, sizeof(double) * nint, s), "ScanGPU")) e = 1;
-	if (!e && nb && post(cudaMallocAsync(&d_bin, sizeof(float) * nb, s), "ScanGPU")) e = 1;
-	if (!e) {
+	// device staging of the positions and results, kept by the context and
+	// grown on demand (no allocation per call once it fits)
+	const size_t o_int = ((sizeof(float) * 2 * npos + 255) / 256) * 256;
+	const size_t o_bin = o_int + ((sizeof(double) * nint + 255) / 256) * 256;
+	const size_t need = o_bin + sizeof(float) * nb;
+	if (need > io_cap_) {
+		if (s) cudaStreamSynchronize(s);
+		dfree(d_io_);
+		io_cap_ = 0;
+		if (post(cudaMalloc(&d_io_, need), "ScanGPU")) return 1;
+		io_cap_ = need;
+	}
+	float* d_pos = reinterpret_cast<float*>(d_io_);
+	double* d_int = nint ? reinterpret_cast<double*>(d_io_ + o_int) : nullptr;
+	float* d_bin = nb ? reinterpret_cast<float*>(d_io_ + o_bin) : nullptr;
+	{
 		cudaMemcpyAsync(d_pos, pos, sizeof(float) * 2 * npos, cudaMemcpyHostToDevice, s);
 		if (d_int) cudaMemsetAsync(d_int, 0, sizeof(double) * nint, s);
 		if (d_bin) cudaMemsetAsync(d_bin, 0, sizeof(float) * nb, s);
@@ -1244,10 +1254,6 @@ int JmsB200::ScanGPU(int npos, const float* pos, float dz, int npass, const int*
 		cudaMemcpyAsync(out_bin, d_bin, sizeof(float) * nb, cudaMemcpyDeviceToHost, s);
 	}
 	if (post(cudaStreamSynchronize(s), "ScanGPU") && !e) e = 201;
-	cudaFreeAsync(d_pos, s);
-	if (d_int) cudaFreeAsync(d_int, s);
-	if (d_bin) cudaFreeAsync(d_bin, s);
-	cudaStreamSynchronize(s);
 	return e;
 }
 

@@ -252,6 +252,8 @@ private:
 	double* d_shiftw_ = nullptr;    // per-wave probe offsets of a fused scan launch
 	size_t shiftw_cap_ = 0;
 	std::vector<int> h_mulw_;
+	uint8_t* d_io_ = nullptr;       // ScanGPU's device staging (positions, sums, binned patterns)
+	size_t io_cap_ = 0;
 	cudaError_t last_cuda_ = cudaSuccess;
 };
 
