@@ -31,19 +31,22 @@
 // FP16 operands carry a power-of-two scale per tile (max |value| -> 2^14),
 // removed exactly after the MMA.
 //
-// Tile.  A CTA of 128 threads owns a tile of T = 4096 points: L = T / N
+// Tile.  A CTA of 512 threads owns a tile of T = 4096 points: L = T / N
 // lines of length N (rows of the wave in the row pass, adjacent columns in
 // the column pass).  Its rows come in two sets:
 //   P: (line l, n2), R1 values each (stage-1 rows), T / R1 rows;
 //   Q: (line l, k1), R2 values each (stage-2 rows), T / R2 rows;
-// thread t owns rows t + 128 j of the current set and reads their D rows
-// from its TMEM lane.  Between the two stages a thread writes its values into
-// the other set's A operand (the transpose of the FFT), through layouts
-// padded so that those writes are free of bank conflicts.  The elementwise
-// step of the pass (x P, or x t) runs in registers between the halves, so a
-// line is read from and written to HBM once per pass, as in the FP32 kernels.
-// The kernels are persistent: one CTA builds the DFT matrices and twiddles in
-// shared memory once and walks its tiles.
+// 4 threads serve each TMEM lane: thread t owns rows t % 128 + 128 j of the
+// current set, holds the quarter t / 128 of their values (8 complex values
+// per thread, 64 registers) and reads that quarter of their D rows from its
+// lane.  Between the two stages a thread writes its values into the other
+// set's A operand (the transpose of the FFT), through layouts padded so that
+// those writes are free of bank conflicts.  The elementwise step of the pass
+// (x P, or x t) runs in registers between the halves, so a line is read from
+// and written to HBM once per pass, as in the FP32 kernels.  The kernels are
+// persistent: a CTA copies the DFT matrices (built once per device) and
+// builds its twiddles in shared memory, then walks its tiles, loading the
+// next tile's input while the MMAs of the current tile's last stage run.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include "jms_fft.cuh"
