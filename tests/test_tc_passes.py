@@ -170,3 +170,52 @@ def test_tc_falls_back_on_unsupported_grid(J):
         J.set_precision(0)
     assert res["fp16"][1] == 0
     assert np.array_equal(res["fp32"][0], res["fp16"][0])
+
+
+@pytest.mark.parametrize("nx,ny", [(512, 256), (256, 1024)])
+def test_tc_non_square_grid_matches_fp32(J, nx, ny):
+    """Non-square grids: the row pass tiles rows of length nx, the column pass
+    columns of length ny, each with its own twiddles and plan.  The BF16
+    tensor-core scan matches the FP32 scan within 1e-4 (integrated signals per
+    detector, binned patterns of their maximum)."""
+    from jmultislicelib_b200 import synthetic as S
+
+    cfg = S.PRECISION_SWEEP
+    a, b = nx * cfg["pixel"], ny * cfg["pixel"]
+    pgr = np.stack([S.random_phase_gratings(nx, ny, a, b, 1, cfg["seed"] + 11 + k)[0] for k in range(2)])
+    nobj = 30
+    J.cleanup()
+    J.set_high_tension(cfg["kv"])
+    J.set_grid(nx, ny, a, b, S.DZ_SLICE)
+    pro = J.calc_propagator(S.DZ_SLICE, 0.0, 0.0, cfg["ntype"])
+    dets = [J.calc_ring_detector(b0, b1) for (b0, b1) in cfg["dets"]]
+    probe = J.calc_probe(cfg["alpha"])
+    objslc = np.arange(nobj) % 2
+    assert J.setup(GPU, [1, 1], objslc, [0, 0], 10, 3, G.INT) == [0, 0, 0, 0]
+    for s_ in range(2):
+        assert J.set_phase_grating(GPU, s_, pgr[s_:s_ + 1]) == 0
+    assert J.set_propagator(GPU, 0, pro) == 0
+    for i, (d, m) in enumerate(dets):
+        assert J.set_detector(GPU, i, d, m) == 0
+    assert J.init_core(GPU) == 0
+    assert J.set_incident_wave(GPU, probe) == 0
+    rng = np.random.default_rng(nx + ny)
+    pos = np.stack([rng.uniform(0, a, 12), rng.uniform(0, b, 12)], axis=1).astype(np.float32)
+    varseq = np.zeros((2, nobj), np.int32)
+    outs = {}
+    for f in ("fp32", "bf16"):
+        assert J.set_precision(MODE[f]) == 0
+        tc0 = J.L.JMS_TcLaunches()
+        e, di, db = J.scan(pos, 2, varseq=varseq, bin=4)
+        assert e == 0, e
+        outs[f] = (di, db, J.L.JMS_TcLaunches() - tc0)
+    assert J.tc_status() == 0
+    J.set_precision(0)
+    J.cleanup()
+    (i0, b0, _), (i1, b1, ntc) = outs["fp32"], outs["bf16"]
+    assert ntc > 0
+    den = np.maximum(np.abs(i0).max(axis=(0, 1)), 1e-30)
+    e_int = float((np.abs(i1 - i0).max(axis=(0, 1)) / den).max())
+    e_bin = float(np.abs(b1 - b0).max() / np.abs(b0).max())
+    assert e_int < BAR_50 and e_bin < BAR_50, (e_int, e_bin)
+
