@@ -230,12 +230,13 @@ int JMS_PlanName(int axis, char* name, int len);
 int JMS_GridSupported(int nx, int ny);
 /* Arithmetic of the line transforms (no counterpart in the reference, whose
  * GPU path is cuFFT in FP32, src/JFFTCUDAcore.cpp:299-336): 0 = FP32 passes
- * (default); 1 = tensor-core passes, each radix-16/32 stage a DFT-matrix
- * product with BF16 hi+lo operands and FP32 accumulation; 2 = the same with
- * FP16 hi+lo operands (power-of-two scaled per tile).  The tensor-core passes
- * serve the slices without readout on grids whose lengths are 256, 512 or
- * 1024; readout slices, sub-frame gratings, plasmon shifts and other lengths
- * run the FP32 passes.  Returns 0, or 1 for a mode out of range. */
+ * (default); 1 = tensor-core passes, each radix-16/32/64 stage a
+ * DFT-matrix product with BF16 hi+lo operands and FP32 accumulation; 2 = the
+ * same with FP16 hi+lo operands (power-of-two scaled per tile).  The
+ * tensor-core passes serve the slices without readout on grids whose lengths
+ * are 256, 512, 1024 or 2048; readout slices, sub-frame gratings, plasmon
+ * shifts and other lengths run the FP32 passes.  Returns 0, or 1 for a mode
+ * out of range. */
 int JMS_SetPrecision(int mode);
 int JMS_GetPrecision(void);
 /* 1 if a tensor-core pass found its matrix products unfinished after its

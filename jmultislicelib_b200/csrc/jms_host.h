@@ -159,7 +159,7 @@ public:
 	// Arithmetic of the line transforms: 0 = FP32 passes (default), 1 = tensor-
 	// core passes with BF16 hi+lo operands, 2 = tensor-core passes with FP16
 	// hi+lo operands (jms_tc.cu).  The tensor-core passes run the steps without
-	// readout for line lengths 256, 512 and 1024; readout steps, sub-frame
+	// readout for line lengths 256, 512, 1024 and 2048; readout steps, sub-frame
 	// gratings, plasmon shifts and other lengths keep the FP32 passes.
 	int SetPrecision(int mode);
 	int GetPrecision() const { return prec_; }

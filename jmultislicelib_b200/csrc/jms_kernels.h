@@ -99,7 +99,7 @@ const PlanOps* plan_get(int n, int idx);
 inline bool pass_supported(int n) { return plan_count(n) > 0; }
 
 // Tensor-core forms of the row and column passes (jms_tc.cu) for line lengths
-// 256, 512 and 1024: prec 1 = BF16 hi+lo operands, 2 = FP16 hi+lo, FP32
+// 256, 512, 1024 and 2048: prec 1 = BF16 hi+lo operands, 2 = FP16 hi+lo, FP32
 // accumulation.  No readout; the column pass needs a grating of the grid size
 // and no plasmon shift.  *err is set to 1 if a tensor-core wait ran out.
 bool tc_supported(int n);

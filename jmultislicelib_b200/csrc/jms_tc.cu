@@ -57,23 +57,24 @@
 namespace jms {
 namespace tc {
 
-constexpr int kTile = 4096;           // complex points per tile
 constexpr int kLanes = 128;           // rows of an MMA tile = TMEM lanes (M = 128)
 constexpr int kQ = 4;                 // threads per TMEM lane: each holds a quarter of its rows' values
 constexpr int kThr = kLanes * kQ;     // threads per CTA
-constexpr int kVal = kTile / kThr;    // complex values per thread
-constexpr int kDCols = 64;            // FP32 accumulator columns of a stage (2 T / 128)
-constexpr int kTmemCols = 2 * kDCols; // main products and correction products in separate accumulators
+// complex points per tile: 4096, or 8192 for N = 2048 (4 lines, so that the
+// 64-point stage's (line, n2) rows still fill M = 128)
+__host__ __device__ constexpr int tile_of(int n) { return n == 2048 ? 8192 : 4096; }
 constexpr long long kMaxWaitCycles = 2000000000LL; // ~1 s at 1.9 GHz, then the pass reports an error
 
 template <int N> struct Radix;
 template <> struct Radix<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Radix<512> { static constexpr int R1 = 32, R2 = 16; };
 template <> struct Radix<1024> { static constexpr int R1 = 32, R2 = 32; };
+template <> struct Radix<2048> { static constexpr int R1 = 64, R2 = 32; };
 
 // (LBO, SBO) of the A layouts of sets P and Q, chosen by a bank-conflict
 // search over the transposing writes (conflict-free except the 256-point
-// column pass, which is 2-way)
+// column passes of 256 and 2048 points, which are 2-way; the conflict-free
+// 2048-point column layout would not fit in shared memory)
 template <int N, bool COL> struct Lay;
 template <> struct Lay<256, false> { static constexpr int lp = 144, sp = 608, lq = 144, sq = 608; };
 template <> struct Lay<512, false> { static constexpr int lp = 144, sp = 1152, lq = 144, sq = 592; };
@@ -81,6 +82,8 @@ template <> struct Lay<1024, false> { static constexpr int lp = 144, sp = 1152, 
 template <> struct Lay<256, true> { static constexpr int lp = 128, sp = 512, lq = 128, sq = 512; };
 template <> struct Lay<512, true> { static constexpr int lp = 128, sp = 1024, lq = 128, sq = 512; };
 template <> struct Lay<1024, true> { static constexpr int lp = 192, sp = 1536, lq = 192, sq = 1536; };
+template <> struct Lay<2048, false> { static constexpr int lp = 144, sp = 2304, lq = 144, sq = 1152; };
+template <> struct Lay<2048, true> { static constexpr int lp = 128, sp = 2048, lq = 128, sq = 1024; };
 
 constexpr int rup(int x, int a) { return (x + a - 1) / a * a; }
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -88,7 +91,11 @@ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 template <int N, bool COL>
 struct Geo {
 	static constexpr int R1 = Radix<N>::R1, R2 = Radix<N>::R2;
-	static constexpr int L = kTile / N;                  // lines per tile
+	static constexpr int T = tile_of(N);                 // points per tile
+	static constexpr int NV = T / kThr;                  // complex values per thread
+	static constexpr int DC = T / 64;                    // FP32 accumulator columns of a stage (J 2R = 2 T / 128)
+	static constexpr int TCOLS = 2 * DC;                 // main + correction accumulators
+	static constexpr int L = T / N;                      // lines per tile
 	static constexpr int MP = L * R2, MQ = L * R1;       // rows of sets P and Q
 	static constexpr int JP = MP / kLanes, JQ = MQ / kLanes; // rows per TMEM lane (and per thread)
 	static constexpr int VP = R1 / kQ, VQ = R2 / kQ;         // values per thread and row in P / Q
@@ -219,17 +226,22 @@ __device__ void build_dft(uint8_t* f)
 // DFT matrices of both radices and operand types, built once per device by
 // k_build_dft (tc_prepare) and copied into shared memory by each CTA:
 // [type (0 BF16, 1 FP16)][R = 16 (6144 B), R = 32 (24576 B)]
-constexpr int kDftType = 3 * 8 * (16 * 16 + 32 * 32);
+constexpr int kDftType = 3 * 8 * (16 * 16 + 32 * 32 + 64 * 64);
 __device__ __align__(16) uint8_t g_dft[2 * kDftType];
-__host__ __device__ constexpr int dft_off(int type, int R) { return type * kDftType + (R == 32 ? 3 * 8 * 16 * 16 : 0); }
+__host__ __device__ constexpr int dft_off(int type, int R)
+{
+	return type * kDftType + (R == 16 ? 0 : R == 32 ? 3 * 8 * 16 * 16 : 3 * 8 * (16 * 16 + 32 * 32));
+}
 
 __global__ void __launch_bounds__(kThr) k_build_dft()
 {
 	switch (blockIdx.x) {
 	case 0: build_dft<16, Bf16>(g_dft + dft_off(0, 16)); break;
 	case 1: build_dft<32, Bf16>(g_dft + dft_off(0, 32)); break;
-	case 2: build_dft<16, Fp16>(g_dft + dft_off(1, 16)); break;
-	default: build_dft<32, Fp16>(g_dft + dft_off(1, 32)); break;
+	case 2: build_dft<64, Bf16>(g_dft + dft_off(0, 64)); break;
+	case 3: build_dft<16, Fp16>(g_dft + dft_off(1, 16)); break;
+	case 4: build_dft<32, Fp16>(g_dft + dft_off(1, 32)); break;
+	default: build_dft<64, Fp16>(g_dft + dft_off(1, 64)); break;
 	}
 }
 
@@ -242,8 +254,8 @@ __device__ __forceinline__ void copy_dft(uint8_t* dst, int type)
 
 // Per-tile power-of-two operand scale (FP16 only): returns s with
 // max |v| * s < 2^14; *inv = 1 / s.  Block-wide (every thread calls it).
-template <class PR>
-__device__ __forceinline__ float tile_scale(const float2 (&v)[kVal], float* red, float* inv)
+template <class PR, int NV>
+__device__ __forceinline__ float tile_scale(const float2 (&v)[NV], float* red, float* inv)
 {
 	if constexpr (!PR::kScale) {
 		*inv = 1.f;
@@ -252,7 +264,7 @@ __device__ __forceinline__ float tile_scale(const float2 (&v)[kVal], float* red,
 	else {
 		float mx = 0.f;
 		#pragma unroll
-		for (int q = 0; q < kVal; q++) mx = fmaxf(mx, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
+		for (int q = 0; q < NV; q++) mx = fmaxf(mx, fmaxf(fabsf(v[q].x), fabsf(v[q].y)));
 		#pragma unroll
 		for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
 		if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
@@ -277,8 +289,8 @@ __device__ __forceinline__ int quarter_of() { return threadIdx.x >> 7; }
 // A operand of a set whose rows are the thread's own rows: row m, 16-byte
 // chunk c = values 4c .. 4c+3 (8 16-bit numbers); the thread writes the
 // chunks of its quarter
-template <int R, int J, int LB, int SB, class PR>
-__device__ __forceinline__ void write_own(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
+template <int R, int J, int LB, int SB, class PR, int NV>
+__device__ __forceinline__ void write_own(const float2 (&v)[NV], uint8_t* ahi, uint8_t* alo, float s)
 {
 	constexpr int V = R / kQ;
 	#pragma unroll
@@ -300,8 +312,8 @@ __device__ __forceinline__ void write_own(const float2 (&v)[kVal], uint8_t* ahi,
 
 // transposing write P -> Q: the thread's P rows (l, n2) hold values over k1
 // (its quarter); Q row (l, k1) gets value n2 at K position n2
-template <class G, class PR>
-__device__ __forceinline__ void write_pq(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
+template <class G, class PR, int NV>
+__device__ __forceinline__ void write_pq(const float2 (&v)[NV], uint8_t* ahi, uint8_t* alo, float s)
 {
 	constexpr int V = G::VP;
 	#pragma unroll
@@ -324,8 +336,8 @@ __device__ __forceinline__ void write_pq(const float2 (&v)[kVal], uint8_t* ahi, 
 
 // transposing write Q -> P: the thread's Q rows (l, k1) hold values over n2
 // (its quarter); P row (l, n2) gets value k1 at K position k1
-template <class G, class PR>
-__device__ __forceinline__ void write_qp(const float2 (&v)[kVal], uint8_t* ahi, uint8_t* alo, float s)
+template <class G, class PR, int NV>
+__device__ __forceinline__ void write_qp(const float2 (&v)[NV], uint8_t* ahi, uint8_t* alo, float s)
 {
 	constexpr int V = G::VQ;
 	#pragma unroll
@@ -348,12 +360,13 @@ __device__ __forceinline__ void write_qp(const float2 (&v)[kVal], uint8_t* ahi, 
 
 // V complex values (2V columns from taddr) of a D row: main accumulator +
 // correction accumulator
-template <int V>
+template <int V, int DC>
 __device__ __forceinline__ void tmem_ld_vals(uint32_t taddr, float2* dst, float inv)
 {
 	uint32_t r[2 * V], c[2 * V];
-	if constexpr (V == 4) { tmem_ld8(taddr, r); tmem_ld8(taddr + kDCols, c); }
-	else { tmem_ld16(taddr, r); tmem_ld16(taddr + kDCols, c); }
+	if constexpr (V == 4) { tmem_ld8(taddr, r); tmem_ld8(taddr + DC, c); }
+	else if constexpr (V == 8) { tmem_ld16(taddr, r); tmem_ld16(taddr + DC, c); }
+	else { tmem_ld32(taddr, r); tmem_ld32(taddr + DC, c); }
 	tmem_wait_ld();
 	#pragma unroll
 	for (int q = 0; q < V; q++)
@@ -370,7 +383,7 @@ __device__ __forceinline__ void tmem_ld_vals(uint32_t taddr, float2* dst, float 
 //   stage_read:  every thread reads its J rows of D (R complex each).
 // Between issue and wait a thread may do work that does not touch A or D
 // (the passes prefetch their next tile there).
-template <int R, int J, int LB, int SB, class PR>
+template <int R, int J, int LB, int SB, class PR, int DC>
 __device__ __forceinline__ void stage_issue(const uint8_t* ahi, const uint8_t* alo, const uint8_t* f, uint32_t tmem,
 	uint32_t mbar)
 {
@@ -393,10 +406,10 @@ __device__ __forceinline__ void stage_issue(const uint8_t* ahi, const uint8_t* a
 				const uint64_t dbl = sdesc(bl + bo, 128, 32 * R);
 				const uint32_t acc = kk > 0 ? 1u : 0u;
 				mma_f16(d, dah, dbh, idesc, acc);
-				mma_f16(d + kDCols, dal, dbh, idesc, acc);
-				mma_f16(d + kDCols, dah, dbm, idesc, 1u);
-				mma_f16(d + kDCols, dal, dbm, idesc, 1u);
-				mma_f16(d + kDCols, dah, dbl, idesc, 1u);
+				mma_f16(d + DC, dal, dbh, idesc, acc);
+				mma_f16(d + DC, dah, dbm, idesc, 1u);
+				mma_f16(d + DC, dal, dbm, idesc, 1u);
+				mma_f16(d + DC, dah, dbl, idesc, 1u);
 			}
 		}
 		mma_commit(mbar);
@@ -424,20 +437,20 @@ __device__ __forceinline__ uint32_t d_addr(uint32_t tmem, int i)
 	return tmem + ((uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16) + (uint32_t)(i * 2 * R + quarter_of() * 2 * (R / kQ));
 }
 
-template <int R, int J>
-__device__ __forceinline__ void stage_read(float2 (&v)[kVal], uint32_t tmem, float inv)
+template <int R, int J, int DC, int NV>
+__device__ __forceinline__ void stage_read(float2 (&v)[NV], uint32_t tmem, float inv)
 {
 	#pragma unroll
-	for (int i = 0; i < J; i++) tmem_ld_vals<R / kQ>(d_addr<R>(tmem, i), &v[i * (R / kQ)], inv);
+	for (int i = 0; i < J; i++) tmem_ld_vals<R / kQ, DC>(d_addr<R>(tmem, i), &v[i * (R / kQ)], inv);
 }
 
-template <int R, int J, int LB, int SB, class PR>
-__device__ __forceinline__ bool stage(float2 (&v)[kVal], const uint8_t* ahi, const uint8_t* alo, const uint8_t* f,
+template <int R, int J, int LB, int SB, class PR, int DC, int NV>
+__device__ __forceinline__ bool stage(float2 (&v)[NV], const uint8_t* ahi, const uint8_t* alo, const uint8_t* f,
 	uint32_t tmem, uint32_t mbar, uint32_t& phase, float inv)
 {
-	stage_issue<R, J, LB, SB, PR>(ahi, alo, f, tmem, mbar);
+	stage_issue<R, J, LB, SB, PR, DC>(ahi, alo, f, tmem, mbar);
 	if (!stage_wait(mbar, phase)) return false;
-	stage_read<R, J>(v, tmem, inv);
+	stage_read<R, J, DC>(v, tmem, inv);
 	return true;
 }
 
@@ -449,10 +462,10 @@ struct TcTiles {
 };
 
 template <int N, bool COL, class PR>
-__global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcTiles tt)
+__global__ void __launch_bounds__(kThr, N == 2048 ? 1 : 2) k_tc_pass(const PassArgs p, const TcTiles tt)
 {
 	using G = Geo<N, COL>;
-	constexpr int R1 = G::R1, R2 = G::R2, L = G::L, VP = G::VP, VQ = G::VQ;
+	constexpr int R1 = G::R1, R2 = G::R2, L = G::L, VP = G::VP, VQ = G::VQ, DC = G::DC;
 	extern __shared__ __align__(1024) uint8_t sm[];
 	__shared__ __align__(8) uint64_t mbar_s;
 	__shared__ uint32_t tbase_s;
@@ -477,14 +490,14 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 	}
 	const uint32_t mbar = smem_u32(&mbar_s);
 	if (tid == 0) mbar_init(mbar, 1);
-	if (tid < 32) tmem_alloc<kTmemCols>(smem_u32(&tbase_s));
+	if (tid < 32) tmem_alloc<G::TCOLS>(smem_u32(&tbase_s));
 	fence_before_sync();
 	__syncthreads();
 	fence_after_sync();
 	const uint32_t tmem = tbase_s;
 	uint32_t phase = 0;
 	bool ok = true;
-	float2 v[kVal];
+	float2 v[G::NV];
 	float inv = 1.f, s = 1.f;
 	// tile t -> wave b and first row (row pass) / column (column pass)
 	auto decode = [&](long long t, int& b, int& first) {
@@ -540,7 +553,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			const int row0 = first;
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR, DC>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
@@ -550,7 +563,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_pq<G, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR, DC>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
 			// Fourier space: x P, then the inverse transform through conj(F(conj(.)))
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
@@ -562,7 +575,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR, DC>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
@@ -572,7 +585,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_qp<G, PR>(v, ahi, alo, s);
-			stage_issue<R1, G::JP, G::LP, G::SP, PR>(ahi, alo, f1, tmem, mbar);
+			stage_issue<R1, G::JP, G::LP, G::SP, PR, DC>(ahi, alo, f1, tmem, mbar);
 			// v is free until the next tile: its loads overlap this last stage
 			if (next < tt.ntiles) load_tile(next);
 			if (!(ok = stage_wait(mbar, phase))) break;
@@ -583,7 +596,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 				const int y = row0 + l;
 				const bool live = y <= p.row_k1 || y >= p.row_k2;
 				float2 d[VP];
-				tmem_ld_vals<VP>(d_addr<R1>(tmem, j), d, inv);
+				tmem_ld_vals<VP, DC>(d_addr<R1>(tmem, j), d, inv);
 				if (live) {
 					float2* dst = W + (long long)y * N + n2 + R2 * (q * VP);
 					#pragma unroll
@@ -597,7 +610,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			const int col0 = first;
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R2, G::JQ, G::LQ, G::SQ, PR, DC>(v, ahi, alo, f2, tmem, mbar, phase, inv))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JQ; j++) {
 				int l, k1;
@@ -607,7 +620,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_qp<G, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR, DC>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
 			// real space: x t, then the forward transform
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
@@ -619,7 +632,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_own<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, s);
-			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
+			if (!(ok = stage<R1, G::JP, G::LP, G::SP, PR, DC>(v, ahi, alo, f1, tmem, mbar, phase, inv))) break;
 			#pragma unroll
 			for (int j = 0; j < G::JP; j++) {
 				int l, n2;
@@ -629,7 +642,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 			}
 			s = tile_scale<PR>(v, red_s, &inv);
 			write_pq<G, PR>(v, ahi, alo, s);
-			stage_issue<R2, G::JQ, G::LQ, G::SQ, PR>(ahi, alo, f2, tmem, mbar);
+			stage_issue<R2, G::JQ, G::LQ, G::SQ, PR, DC>(ahi, alo, f2, tmem, mbar);
 			// v is free until the next tile: its loads overlap this last stage
 			if (next < tt.ntiles) load_tile(next);
 			if (!(ok = stage_wait(mbar, phase))) break;
@@ -638,7 +651,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 				int l, k1;
 				G::qinv(lane + kLanes * j, l, k1);
 				float2 d[VQ];
-				tmem_ld_vals<VQ>(d_addr<R2>(tmem, j), d, inv);
+				tmem_ld_vals<VQ, DC>(d_addr<R2>(tmem, j), d, inv);
 				const int k20 = q * VQ;
 				float2* dst = W + col0 + (k1 + R1 * k20) * nx + l;
 				#pragma unroll
@@ -651,7 +664,7 @@ __global__ void __launch_bounds__(kThr, 2) k_tc_pass(const PassArgs p, const TcT
 	}
 	fence_before_sync();
 	__syncthreads();
-	if (tid < 32) tmem_dealloc<kTmemCols>(tmem);
+	if (tid < 32) tmem_dealloc<G::TCOLS>(tmem);
 	if (!ok && tid == 0 && tt.err) atomicExch(tt.err, 1);
 }
 
@@ -671,7 +684,7 @@ cudaError_t launch(const PassArgs& p, TcTiles tt, cudaStream_t s)
 		if (e != cudaSuccess) return e;
 		int nsm = 0, per_sm = 1;
 		cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-		e = resident_ctas(kern, kThr, G::kSmem, 512 / kTmemCols, &per_sm); // TMEM: 512 columns per SM
+		e = resident_ctas(kern, kThr, G::kSmem, 512 / G::TCOLS, &per_sm); // TMEM: 512 columns per SM
 		if (e != cudaSuccess) return e;
 		grid = nsm * per_sm;
 	}
@@ -688,17 +701,18 @@ cudaError_t dispatch(int n, const PassArgs& p, const TcTiles& tt, int prec, cuda
 	case 256: return f16 ? launch<256, COL, Fp16>(p, tt, s) : launch<256, COL, Bf16>(p, tt, s);
 	case 512: return f16 ? launch<512, COL, Fp16>(p, tt, s) : launch<512, COL, Bf16>(p, tt, s);
 	case 1024: return f16 ? launch<1024, COL, Fp16>(p, tt, s) : launch<1024, COL, Bf16>(p, tt, s);
+	case 2048: return f16 ? launch<2048, COL, Fp16>(p, tt, s) : launch<2048, COL, Bf16>(p, tt, s);
 	default: return cudaErrorInvalidValue;
 	}
 }
 
 } // namespace tc
 
-bool tc_supported(int n) { return n == 256 || n == 512 || n == 1024; }
+bool tc_supported(int n) { return n == 256 || n == 512 || n == 1024 || n == 2048; }
 
 cudaError_t tc_prepare(cudaStream_t s)
 {
-	tc::k_build_dft<<<4, tc::kThr, 0, s>>>();
+	tc::k_build_dft<<<6, tc::kThr, 0, s>>>();
 	cudaError_t e = cudaGetLastError();
 	if (e != cudaSuccess) return e;
 	return cudaStreamSynchronize(s);
@@ -707,7 +721,7 @@ cudaError_t tc_prepare(cudaStream_t s)
 cudaError_t launch_tc_row(const PassArgs& p, int prec, int* err, cudaStream_t s)
 {
 	if (!tc_supported(p.nx) || prec < 1 || prec > 2) return cudaErrorInvalidValue;
-	const int L = tc::kTile / p.nx;
+	const int L = tc::tile_of(p.nx) / p.nx;
 	if (p.ny % L) return cudaErrorInvalidValue;
 	const int nrb = p.ny / L;
 	int split = nrb, skip = 0;
@@ -729,7 +743,7 @@ cudaError_t launch_tc_col(const PassArgs& p, int prec, int* err, cudaStream_t s)
 {
 	if (!tc_supported(p.ny) || prec < 1 || prec > 2) return cudaErrorInvalidValue;
 	if (p.npgx != p.nx || p.npgy != p.ny) return cudaErrorInvalidValue;
-	const int L = tc::kTile / p.ny;
+	const int L = tc::tile_of(p.ny) / p.ny;
 	if (p.nx % L) return cudaErrorInvalidValue;
 	tc::TcTiles tt;
 	tt.per_wave = p.nx / L;
