@@ -89,8 +89,12 @@ __host__ __device__ constexpr double cx_sin_turn(long num, long den)
 // ---------------------------------------------------------------------------
 // complex helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add and subtract as one packed FP32x2 instruction each (sm_100:
+// add.f32x2 / fma.f32x2, both lanes rounded to nearest like the scalar
+// forms).  a - b is formed as fma(b, -1, a): b * -1 is exact, so the result is
+// the correctly rounded difference.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
 	return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));

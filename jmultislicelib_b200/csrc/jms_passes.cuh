@@ -182,7 +182,7 @@ __device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const fl
 		float2 o;
 		o.x = __shfl_xor_sync(0xffffffffu, u.x, Tile::kPartner);
 		o.y = __shfl_xor_sync(0xffffffffu, u.y, Tile::kPartner);
-		v[k] = make_float2(fmaf(sgn, u.x, o.x), fmaf(sgn, u.y, o.y));
+		v[k] = __ffma2_rn(make_float2(sgn, sgn), u, o);
 	});
 	__syncthreads();
 }
@@ -204,7 +204,7 @@ __device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const fl
 		float2 o;
 		o.x = __shfl_xor_sync(0xffffffffu, v[k].x, Tile::kPartner);
 		o.y = __shfl_xor_sync(0xffffffffu, v[k].y, Tile::kPartner);
-		const float2 d = make_float2(fmaf(sgn, v[k].x, o.x), fmaf(sgn, v[k].y, o.y));
+		const float2 d = __ffma2_rn(make_float2(sgn, sgn), v[k], o);
 		v[k] = h ? twiddle_ct<k, B, INV>(d) : d;
 	});
 	dft_reg<A, 1, 0, INV>(v);   // output q2 = 2 m + h
@@ -384,8 +384,8 @@ __device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y,
 	const long long c = (long long)b * p.chan_wstride + (long long)p.plane * N + idx;
 	if (p.dif) p.dif[c] += p.weight * pw;
 	if (p.dif_avg) p.dif_avg[c] += p.weight * pw;
-	if (p.wff) p.wff[c] = cadd(p.wff[c], cscale(v, p.weight));
-	if (p.wff_avg) p.wff_avg[c] = cadd(p.wff_avg[c], cscale(v, p.weight));
+	if (p.wff) p.wff[c] = __ffma2_rn(v, make_float2(p.weight, p.weight), p.wff[c]);
+	if (p.wff_avg) p.wff_avg[c] = __ffma2_rn(v, make_float2(p.weight, p.weight), p.wff_avg[c]);
 	if (p.bin_out && p.plane == p.bin_plane) {
 		// unscrambled position (zero beam at nx/2, ny/2 as GetUnscrambleHash,
 		// src/JMultiSlice.cpp:1932-1958), then bin x bin pixel blocks
@@ -406,8 +406,8 @@ __device__ __forceinline__ void readout_real(const PassArgs& p, int b, int y, in
 	const float pw = cnorm(v);
 	if (p.img) p.img[c] += p.weight * pw;
 	if (p.img_avg) p.img_avg[c] += p.weight * pw;
-	if (p.wfr) p.wfr[c] = cadd(p.wfr[c], cscale(v, p.weight));
-	if (p.wfr_avg) p.wfr_avg[c] = cadd(p.wfr_avg[c], cscale(v, p.weight));
+	if (p.wfr) p.wfr[c] = __ffma2_rn(v, make_float2(p.weight, p.weight), p.wfr[c]);
+	if (p.wfr_avg) p.wfr_avg[c] = __ffma2_rn(v, make_float2(p.weight, p.weight), p.wfr_avg[c]);
 }
 
 // offset phase plate exp(-i (2 pi turns + cppl)) at scrambled pixel (i, j);
