@@ -49,19 +49,28 @@ cudaError_t launch_pgr_sites(double2* pos, const double2* base, const double* ux
 // ---------------------------------------------------------------------------
 // Fourier synthesis of the projected potential
 // ---------------------------------------------------------------------------
-// A CTA owns a 32 x 32 pixel tile of one grating: thread (x = lane, group)
-// accumulates 4 rows of one column.  The translation phase is separable,
-// exp(-2 pi i (x qx + y qy)) = ex(qx) ey(qy); per chunk of 32 atoms the CTA
-// tabulates ex for its 32 columns and occ * ey for its 32 rows in shared
-// memory (64 sincos per atom instead of 1024), the phase in turns x/a * fi
-// formed in FP64 and reduced to [-1/2, 1/2) before the FP32 sincospi.
+// The structure factor S_t(q) = sum_a occ_a exp(-2 pi i (x_a qx + y_a qy))
+// is separable per atom, exp(-2 pi i (x qx + y qy)) = ex(qx) ey(qy), so the
+// synthesis runs on tables made once per call:
+//   k_pgr_phase: ex of every atom and column, occ * ey of every atom and row,
+//                the phase in turns x/a * fi formed in FP64 and reduced to
+//                [-1/2, 1/2) before the FP32 sincospi;
+//   k_pgr_fq:    f_t(|q|) (times ap(q)^2 under bwl_pot) of every type and
+//                pixel, once per setup;
+//   k_pgr_synth: a CTA owns a 64 x 64 pixel tile of one grating; thread
+//                (lane, warp) keeps S of columns 2 lane, 2 lane + 1 and rows
+//                8 warp ... +7 in registers (64 FMAs per atom against 5
+//                shared loads).
+// Every output sums its atoms in type order, then atom order, with two FMAs
+// per component and atom, and adds f_t S_t over the types in order.
 namespace {
-constexpr int kSX = 32, kSG = 8, kSR = 4, kSY = kSG * kSR, kCH = 32;
+constexpr int kSX = 64, kSY = 64, kRW = 8, kCH = 32, kSThr = 256;
+constexpr int kChunkF2 = kCH * (kSX + kSY);     // float2 per staged chunk: ex [kCH][kSX], then ey [kCH][kSY]
 
+// signed frequency index of bin i < n: 0, 1, ..., then -floor(n/2), ..., -1
 __device__ __forceinline__ int freq(int i, int n)
 {
-	const int h = (n - (n % 2)) >> 1;
-	return ((i + h) % n) - h;
+	return i < n - (n >> 1) ? i : i - n;
 }
 
 __device__ __forceinline__ float2 cis_turns_neg(double t)
@@ -71,90 +80,212 @@ __device__ __forceinline__ float2 cis_turns_neg(double t)
 	sincospif(2.f * (float)t, &s, &c);
 	return make_float2(c, -s);
 }
+
+// S += e * w (complex)
+__device__ __forceinline__ void cmac(float2& S, float ex, float ey, float wx, float wy)
+{
+	S.x = fmaf(ex, wx, fmaf(-ey, wy, S.x));
+	S.y = fmaf(ex, wy, fmaf(ey, wx, S.y));
+}
+
+// 8-byte asynchronous copy global -> shared; valid = false writes zeros
+// (cp_async_commit: jms_passes.cuh)
+__device__ __forceinline__ void cp_async8(float2* dst, const float2* src, bool valid)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_n() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 } // namespace
 
-__global__ void __launch_bounds__(kSX * kSG) k_pgr_synth(const PgrArgs p)
+__global__ void k_pgr_phase(const PgrArgs p, int nb)
 {
-	__shared__ float2 ex[kCH][kSX];
-	__shared__ float2 ey[kCH][kSY];
-	const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5, g = blockIdx.z;
-	const int ix = blockIdx.x * kSX + lane;
-	const int iy0 = blockIdx.y * kSY;
-	const double2* pos = p.site_pos + (long long)g * p.nsite;
-	const float qx = (float)freq(ix < p.nx ? ix : 0, p.nx) * p.itogx;
-	float2 pot[kSR];
-	#pragma unroll
-	for (int r = 0; r < kSR; r++) pot[r] = make_float2(0.f, 0.f);
-	for (int t = 0; t < p.ntype; t++) {
-		float2 S[kSR];
-		#pragma unroll
-		for (int r = 0; r < kSR; r++) S[r] = make_float2(0.f, 0.f);
-		const int a0 = p.type_start[t], a1 = p.type_start[t + 1];
-		for (int c0 = a0; c0 < a1; c0 += kCH) {
-			const int na = min(kCH, a1 - c0);
-			__syncthreads();
-			for (int k = threadIdx.x; k < na * (kSX + kSY); k += kSX * kSG) {
-				const int a = k / (kSX + kSY), r = k % (kSX + kSY);
-				const int at = c0 + a;
-				const double2 fp = pos[p.atom_site[at]];
-				if (r < kSX) {
-					const int i = blockIdx.x * kSX + r;
-					ex[a][r] = cis_turns_neg(fp.x * (double)freq(i < p.nx ? i : 0, p.nx));
-				}
-				else {
-					const int j = iy0 + r - kSX;
-					const float2 e = cis_turns_neg(fp.y * (double)freq(j < p.ny ? j : 0, p.ny));
-					const float o = p.atom_occ[at];
-					ey[a][r - kSX] = make_float2(o * e.x, o * e.y);
-				}
-			}
-			__syncthreads();
-			for (int a = 0; a < na; a++) {
-				const float2 e = ex[a][lane];
-				#pragma unroll
-				for (int r = 0; r < kSR; r++) {
-					const float2 w = ey[a][grp * kSR + r];     // broadcast
-					S[r].x = fmaf(e.x, w.x, fmaf(-e.y, w.y, S[r].x));
-					S[r].y = fmaf(e.x, w.y, fmaf(e.y, w.x, S[r].y));
-				}
-			}
-		}
-		// pot += f_t(|q|) ap1(q)^2 S_t(q)
-		const float2* ff = p.ff + (long long)t * p.nk;
-		#pragma unroll
-		for (int r = 0; r < kSR; r++) {
-			const int iy = iy0 + grp * kSR + r;
-			const float qy = (float)freq(iy < p.ny ? iy : 0, p.ny) * p.itogy;
-			const float q = sqrtf(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qy, qy)));
-			const float fpq = q / p.sk;
-			int i0 = (int)fpq;
-			i0 = min(i0, p.nk - 2);
-			const float w1 = fpq - (float)i0;
-			const float2 f0 = __ldg(ff + i0), f1 = __ldg(ff + i0 + 1);
-			float fr = f0.x * (1.f - w1) + f1.x * w1;
-			float fi = f0.y * (1.f - w1) + f1.y * w1;
-			if (p.bwl_pot) {
-				const float ap = 0.5f - 0.5f * tanhf((q / p.kmax - 0.9f) * 30.f);
-				fr *= ap * ap;
-				fi *= ap * ap;
-			}
-			pot[r].x += fr * S[r].x - fi * S[r].y;
-			pot[r].y += fr * S[r].y + fi * S[r].x;
-		}
+	const int a = blockIdx.x / nb, g = blockIdx.z;
+	const int i = (blockIdx.x - a * nb) * blockDim.x + threadIdx.x;
+	if (i >= p.nx + p.ny) return;
+	const double2 fp = p.site_pos[(long long)g * p.nsite + p.atom_site[a]];
+	if (i < p.nx) {
+		p.tx[((long long)g * p.natom + a) * p.nx + i] = cis_turns_neg(fp.x * (double)freq(i, p.nx));
 	}
+	else {
+		const int j = i - p.nx;
+		const float2 e = cis_turns_neg(fp.y * (double)freq(j, p.ny));
+		const float o = p.atom_occ[a];
+		p.ty[((long long)g * p.natom + a) * p.ny + j] = make_float2(o * e.x, o * e.y);
+	}
+}
+
+cudaError_t launch_pgr_phase(const PgrArgs& p, cudaStream_t s)
+{
+	if (p.natom <= 0 || p.ngr <= 0) return cudaSuccess;
+	const int nb = (p.nx + p.ny + 255) / 256;
+	k_pgr_phase<<<dim3((unsigned)(nb * p.natom), 1, p.ngr), 256, 0, s>>>(p, nb);
+	return cudaGetLastError();
+}
+
+__global__ void k_pgr_fq(const PgrArgs p, float2* fq)
+{
+	const int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y, t = blockIdx.z;
 	if (ix >= p.nx) return;
+	const float qx = (float)freq(ix, p.nx) * p.itogx;
+	const float qy = (float)freq(iy, p.ny) * p.itogy;
+	const float q = sqrtf(__fadd_rn(__fmul_rn(qx, qx), __fmul_rn(qy, qy)));
+	const float fpq = q / p.sk;
+	int i0 = (int)fpq;
+	i0 = min(i0, p.nk - 2);
+	const float w1 = fpq - (float)i0;
+	const float2* ff = p.ff + (long long)t * p.nk;
+	const float2 f0 = __ldg(ff + i0), f1 = __ldg(ff + i0 + 1);
+	float fr = f0.x * (1.f - w1) + f1.x * w1;
+	float fi = f0.y * (1.f - w1) + f1.y * w1;
+	if (p.bwl_pot) {
+		const float ap = 0.5f - 0.5f * tanhf((q / p.kmax - 0.9f) * 30.f);
+		fr *= ap * ap;
+		fi *= ap * ap;
+	}
+	fq[((long long)t * p.ny + iy) * p.nx + ix] = make_float2(fr, fi);
+}
+
+cudaError_t launch_pgr_fq(const PgrArgs& p, float2* fq, cudaStream_t s)
+{
+	k_pgr_fq<<<dim3((p.nx + 255) / 256, p.ny, p.ntype), 256, 0, s>>>(p, fq);
+	return cudaGetLastError();
+}
+
+// Chunks of 32 consecutive atoms (type order, across type boundaries) are
+// staged by cp.async into one of two shared buffers while the previous chunk
+// is summed; when a type's atoms end, its f_t S_t joins the potential, which
+// each thread keeps in 16 shared slots (registers hold only S).
+__global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
+{
+	extern __shared__ __align__(16) float2 smem[];     // 2 x kChunkF2 staging, then pot [16][kSThr]
+	float2* pot = smem + 2 * kChunkF2 + threadIdx.x;   // slot k at pot[k * kSThr]
+	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = blockIdx.z;
+	const int ix0 = blockIdx.x * kSX + 2 * lane;
+	const int iy0 = blockIdx.y * kSY + kRW * wp;
+	const float2* txg = p.tx + (long long)g * p.natom * p.nx;
+	const float2* tyg = p.ty + (long long)g * p.natom * p.ny;
+	const int natom = p.natom;
+	const int nch = (natom + kCH - 1) / kCH;
+	// staging: thread k copies table column / row r = k mod 128 of atoms
+	// 2 m + k / 128 of a chunk (m < 16); ex [kCH][kSX] then ey [kCH][kSY]
+	static_assert(kSX == kSY && kSThr == 2 * (kSX + kSY), "staging map");
+	const int sr = threadIdx.x % (kSX + kSY), sa = threadIdx.x / (kSX + kSY);
+	const bool sx = sr < kSX;
+	const int sij = sx ? blockIdx.x * kSX + sr : blockIdx.y * kSY + sr - kSX;
+	const bool sin = sx ? sij < p.nx : sij < p.ny;
+	const float2* ssrc = (sx ? txg : tyg) + (sin ? sij : 0);
+	const int sstr = sx ? p.nx : p.ny;
+	const int sdst = (sx ? sr : kCH * kSX + sr - kSX) + sa * kSX;
+	auto stage = [&](int c) {
+		float2* buf = smem + (c & 1) * kChunkF2 + sdst;
+		#pragma unroll 4
+		for (int m = 0; m < kCH / 2; m++) {
+			const int at = c * kCH + sa + 2 * m;
+			const bool ok = sin && at < natom;
+			cp_async8(buf + 2 * m * kSX, ok ? ssrc + (long long)at * sstr : ssrc, ok);
+		}
+		cp_async_commit();
+	};
+	float2 S[kRW][2];
+	#pragma unroll
+	for (int r = 0; r < kRW; r++) {
+		S[r][0] = S[r][1] = make_float2(0.f, 0.f);
+		pot[(2 * r) * kSThr] = pot[(2 * r + 1) * kSThr] = make_float2(0.f, 0.f);
+	}
+	// pot += f_t(|q|) ap(q)^2 S_t(q); S = 0
+	auto close_type = [&](int t) {
+		const float2* F = p.fq + (long long)t * p.nx * p.ny;
+		#pragma unroll
+		for (int r = 0; r < kRW; r++) {
+			const int iy = iy0 + r;
+			#pragma unroll
+			for (int c = 0; c < 2; c++) {
+				const int ix = ix0 + c;
+				const float2 f = (ix < p.nx && iy < p.ny) ? __ldg(F + (long long)iy * p.nx + ix) : make_float2(0.f, 0.f);
+				const float fr = f.x, fi = f.y;
+				float2 pv = pot[(2 * r + c) * kSThr];
+				pv.x += fr * S[r][c].x - fi * S[r][c].y;
+				pv.y += fr * S[r][c].y + fi * S[r][c].x;
+				pot[(2 * r + c) * kSThr] = pv;
+				S[r][c] = make_float2(0.f, 0.f);
+			}
+		}
+	};
+	int t = 0, tend = p.type_start[1];
+	while (t < p.ntype && tend == 0) { close_type(t); t++; if (t < p.ntype) tend = p.type_start[t + 1]; }
+	if (nch > 0) stage(0);
+	for (int c = 0; c < nch; c++) {
+		if (c + 1 < nch) {
+			stage(c + 1);
+			cp_async_wait_n<1>();
+		}
+		else {
+			cp_async_wait_n<0>();
+		}
+		__syncthreads();
+		const float2* buf = smem + (c & 1) * kChunkF2;
+		const int a0 = c * kCH, a1 = min(natom, a0 + kCH);
+		int a = a0;
+		while (a < a1) {
+			const int aend = min(a1, tend);
+			const float4* pe = reinterpret_cast<const float4*>(buf) + lane + (a - a0) * (kSX / 2);
+			const float4* pw = reinterpret_cast<const float4*>(buf + kCH * kSX) + (kRW / 2) * wp + (a - a0) * (kSY / 2);
+			#pragma unroll 2
+			for (int n = aend - a; n > 0; n--, pe += kSX / 2, pw += kSY / 2) {
+				const float4 e = *pe;                     // columns 2 lane, 2 lane + 1
+				#pragma unroll
+				for (int rr = 0; rr < kRW / 2; rr++) {
+					const float4 w = pw[rr];              // rows 2 rr, 2 rr + 1 (broadcast)
+					cmac(S[2 * rr][0], e.x, e.y, w.x, w.y);
+					cmac(S[2 * rr][1], e.z, e.w, w.x, w.y);
+					cmac(S[2 * rr + 1][0], e.x, e.y, w.z, w.w);
+					cmac(S[2 * rr + 1][1], e.z, e.w, w.z, w.w);
+				}
+			}
+			a = aend;
+			// types whose atoms end here (and empty types after them)
+			while (t < p.ntype && a == tend) {
+				close_type(t);
+				t++;
+				if (t < p.ntype) tend = p.type_start[t + 1];
+			}
+		}
+		__syncthreads();   // the buffer of chunk c is restaged for chunk c + 2
+	}
 	float2* out = p.out + (long long)g * p.gstride;
 	#pragma unroll
-	for (int r = 0; r < kSR; r++) {
-		const int iy = iy0 + grp * kSR + r;
-		if (iy < p.ny) out[(long long)iy * p.nx + ix] = pot[r];
+	for (int r = 0; r < kRW; r++) {
+		const int iy = iy0 + r;
+		if (iy >= p.ny) break;
+		float2* o = out + (long long)iy * p.nx + ix0;
+		const float2 v0 = pot[(2 * r) * kSThr], v1 = pot[(2 * r + 1) * kSThr];
+		if (ix0 + 1 < p.nx && (p.nx & 1) == 0)
+			*reinterpret_cast<float4*>(o) = make_float4(v0.x, v0.y, v1.x, v1.y);
+		else {
+			if (ix0 < p.nx) o[0] = v0;
+			if (ix0 + 1 < p.nx) o[1] = v1;
+		}
 	}
 }
 
 cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s)
 {
+	constexpr int smem = (2 * kChunkF2 + 2 * kRW * kSThr) * (int)sizeof(float2);
+	// the dynamic shared-memory limit is raised once per device
+	static bool attr_set[64] = {};
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess) return e;
+	if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+	if (!attr_set[dev]) {
+		e = cudaFuncSetAttribute(k_pgr_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+		if (e != cudaSuccess) return e;
+		attr_set[dev] = true;
+	}
 	const dim3 grid((p.nx + kSX - 1) / kSX, (p.ny + kSY - 1) / kSY, p.ngr);
-	k_pgr_synth<<<grid, kSX * kSG, 0, s>>>(p);
+	k_pgr_synth<<<grid, kSThr, smem, s>>>(p);
 	return cudaGetLastError();
 }
 

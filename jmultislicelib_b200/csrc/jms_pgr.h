@@ -46,6 +46,13 @@ struct PgrArgs {
 	float itogx = 0.f, itogy = 0.f;     // 1/a, 1/b as the reference's float helpers
 	float kmax = 0.f;                   // min(nyq_x / a, nyq_y / b)
 	int bwl_pot = 0;
+	// precomputed tables of the synthesis: f_t(|q|) ap(q)^2 per type and pixel
+	// [ntype][ny][nx]; translation phases per grating and atom (atoms in type
+	// order), ex [ngr][natom][nx] and occ * ey [ngr][natom][ny]
+	const float2* fq = nullptr;
+	float2* tx = nullptr;
+	float2* ty = nullptr;
+	int natom = 0;
 	// potential -> grating
 	double cphase = 0.0;                // c of t = exp(i c V')
 	const float2* twx = nullptr;
@@ -57,6 +64,11 @@ struct PgrArgs {
 // seed, g, s; Box-Muller).
 cudaError_t launch_pgr_sites(double2* pos, const double2* base, const double* ux_frac, const double* uy_frac,
 	int nsite, int ngr, unsigned long long seed, cudaStream_t s);
+// fq[t][iy][ix] = f_t(|q|) (ap(q)^2 with bwl_pot) for the grid and form factors of p
+cudaError_t launch_pgr_fq(const PgrArgs& p, float2* fq, cudaStream_t s);
+// translation-phase tables p.tx, p.ty of the p.ngr gratings at p.site_pos
+cudaError_t launch_pgr_phase(const PgrArgs& p, cudaStream_t s);
+// potential spectra of p.ngr gratings from the tables p.fq, p.tx, p.ty
 cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s);
 
 // transforms with the default plan of the length (nx for rows, ny for columns)

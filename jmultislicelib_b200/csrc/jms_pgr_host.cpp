@@ -76,9 +76,12 @@ void PgrGen::Reset()
 {
 	ClearSites();
 	dfree(d_ff_); dfree(d_twx_); dfree(d_twy_); dfree(d_ap2_); dfree(d_buf_); dfree(d_out_); dfree(d_pos_);
+	dfree(d_fq_); dfree(d_tab_);
 	d_ff_ = nullptr; d_twx_ = d_twy_ = d_ap2_ = d_buf_ = d_out_ = nullptr;
 	d_pos_ = nullptr;
-	cap_buf_ = cap_out_ = cap_pos_ = 0;
+	d_fq_ = d_tab_ = nullptr;
+	fq_valid_ = false;
+	cap_buf_ = cap_out_ = cap_pos_ = cap_tab_ = 0;
 	status_ = 0;
 	nx_ = ny_ = 0;
 	ntype_ = nk_ = 0;
@@ -92,6 +95,7 @@ int PgrGen::SetGrid(int nx, int ny, float a, float b)
 	ClearSites();
 	dfree(d_twx_); dfree(d_twy_); dfree(d_ap2_);
 	d_twx_ = d_twy_ = d_ap2_ = nullptr;
+	fq_valid_ = false;
 	nx_ = nx; ny_ = ny; a_ = a; b_ = b;
 	std::vector<float2> tw;
 	twiddles(tw, nx);
@@ -126,6 +130,7 @@ int PgrGen::SetPhysics(float ekv, int thermal, int bwl_pot, int bwl_pgr)
 {
 	if (!(ekv > 0.f) || thermal < 0 || thermal > 2) return 1;
 	ClearSites();
+	fq_valid_ = false;
 	ekv_ = ekv;
 	thermal_ = thermal;
 	bwl_pot_ = bwl_pot ? 1 : 0;
@@ -142,6 +147,7 @@ int PgrGen::SetFormFactors(int ntype, int nk, float sk, const float* ff, const f
 {
 	if (ntype < 1 || nk < 2 || !(sk > 0.f) || ff == nullptr) return 1;
 	ClearSites();
+	fq_valid_ = false;
 	dfree(d_ff_);
 	d_ff_ = nullptr;
 	if (cudaMalloc(&d_ff_, sizeof(float2) * (size_t)ntype * nk) != cudaSuccess) return 4;
@@ -301,7 +307,32 @@ int PgrGen::Calculate(int natom, const float* atoms, float cz, int ngr, unsigned
 		if ((e = dput(d_pos_, cap_pos_, (const double2*)nullptr, (size_t)ngr * nsite_, s))) return e;
 		if (launch_pgr_sites(d_pos_, set->base, set->ux, set->uy, nsite_, ngr, seed, s) != cudaSuccess) return 6;
 		p.site_pos = d_pos_;
-		if (launch_pgr_synth(p, s) != cudaSuccess) return 6;
+		if (!fq_valid_) {
+			// the fq table lives as long as the setup: sized once per grid and type count
+			dfree(d_fq_);
+			d_fq_ = nullptr;
+			if (cudaMalloc(&d_fq_, sizeof(float2) * (size_t)ntype_ * N) != cudaSuccess) return 4;
+			if (launch_pgr_fq(p, d_fq_, s) != cudaSuccess) return 6;
+			fq_valid_ = true;
+		}
+		p.fq = d_fq_;
+		p.natom = natom_;
+		// phase tables in groups of gratings of at most 64 MiB (L2-resident
+		// while the synthesis reads each entry once per tile)
+		const size_t per = (size_t)natom_ * (size_t)(nx_ + ny_);
+		const int ng = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(ngr, 65535),
+			((size_t)64 << 20) / (sizeof(float2) * std::max<size_t>(per, 1))));
+		if ((e = dput(d_tab_, cap_tab_, (const float2*)nullptr, per * ng, s))) return e;
+		for (int g0 = 0; g0 < ngr; g0 += ng) {
+			PgrArgs q = p;
+			q.ngr = std::min(ng, ngr - g0);
+			q.site_pos = d_pos_ + (size_t)g0 * nsite_;
+			q.out = d_buf_ + (size_t)g0 * N;
+			q.tx = d_tab_;
+			q.ty = d_tab_ + (size_t)natom_ * nx_ * q.ngr;
+			if (launch_pgr_phase(q, s) != cudaSuccess) return 6;
+			if (launch_pgr_synth(q, s) != cudaSuccess) return 6;
+		}
 		if (launch_pgr_rows_inv(p, s) != cudaSuccess) return 6;
 	}
 	else if (cudaMemsetAsync(d_buf_, 0, sizeof(float2) * ngr * N, s) != cudaSuccess) {

@@ -70,6 +70,12 @@ private:
 	float2 *d_twx_ = nullptr, *d_twy_ = nullptr, *d_ap2_ = nullptr, *d_buf_ = nullptr, *d_out_ = nullptr;
 	double2* d_pos_ = nullptr;
 	size_t cap_buf_ = 0, cap_out_ = 0, cap_pos_ = 0;
+	// synthesis tables: f_t(|q|) per type and pixel (valid while grid, physics
+	// and form factors are unchanged), translation phases per grating group
+	float2* d_fq_ = nullptr;
+	bool fq_valid_ = false;
+	float2* d_tab_ = nullptr;
+	size_t cap_tab_ = 0;
 };
 
 } // namespace jms
