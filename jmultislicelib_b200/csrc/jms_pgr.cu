@@ -60,11 +60,18 @@ cudaError_t launch_pgr_sites(double2* pos, const double2* base, const double* ux
 //   k_pgr_synth: a CTA owns a 64 x 64 pixel tile of one grating; thread
 //                (lane, warp) keeps S of columns 2 lane, 2 lane + 1 and rows
 //                8 warp ... +7 in registers (64 FMAs per atom against 5
-//                shared loads).
+//                shared loads).  Real occupancies make S Hermitian,
+//                S(-q) = conj(S(q)): tiles cover rows iy < ceil(ny / 2) and
+//                also write f_t conj(S_t) at the mirrored pixel
+//                (ny - iy, (nx - ix) mod nx);
+//   k_pgr_lines: the pixels without a sampled mirror, summed directly: the
+//                Nyquist row ny / 2 (even ny) and the Nyquist column nx / 2
+//                of the mirrored rows (even nx), where the grid samples -n/2
+//                and not its partner +n/2.
 // Every output sums its atoms in type order, then atom order, with two FMAs
 // per component and atom, and adds f_t S_t over the types in order.
 namespace {
-constexpr int kSX = 64, kSY = 64, kRW = 8, kCH = 32, kSThr = 256;
+constexpr int kSX = 64, kSY = 64, kRW = 8, kCH = 16, kSThr = 256;
 constexpr int kChunkF2 = kCH * (kSX + kSY);     // float2 per staged chunk: ex [kCH][kSX], then ey [kCH][kSY]
 
 // signed frequency index of bin i < n: 0, 1, ..., then -floor(n/2), ..., -1
@@ -153,15 +160,17 @@ cudaError_t launch_pgr_fq(const PgrArgs& p, float2* fq, cudaStream_t s)
 	return cudaGetLastError();
 }
 
-// Chunks of 32 consecutive atoms (type order, across type boundaries) are
+// Chunks of 16 consecutive atoms (type order, across type boundaries) are
 // staged by cp.async into one of two shared buffers while the previous chunk
-// is summed; when a type's atoms end, its f_t S_t joins the potential, which
-// each thread keeps in 16 shared slots (registers hold only S).
+// is summed; when a type's atoms end, f_t S_t and f_t conj(S_t) join the
+// potentials at q and -q, which each thread keeps in 32 shared slots
+// (registers hold only S).
 __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 {
-	extern __shared__ __align__(16) float2 smem[];     // 2 x kChunkF2 staging, then pot [16][kSThr]
-	float2* pot = smem + 2 * kChunkF2 + threadIdx.x;   // slot k at pot[k * kSThr]
+	extern __shared__ __align__(16) float2 smem[];     // 2 x kChunkF2 staging, then pot [32][kSThr]
+	float2* pot = smem + 2 * kChunkF2 + threadIdx.x;   // slot k (q) and 16 + k (-q) at pot[slot * kSThr]
 	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = blockIdx.z;
+	const int hb = (p.ny + 1) >> 1;                    // rows summed here: iy < hb
 	const int ix0 = blockIdx.x * kSX + 2 * lane;
 	const int iy0 = blockIdx.y * kSY + kRW * wp;
 	const float2* txg = p.tx + (long long)g * p.natom * p.nx;
@@ -169,18 +178,18 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 	const int natom = p.natom;
 	const int nch = (natom + kCH - 1) / kCH;
 	// staging: thread k copies table column / row r = k mod 128 of atoms
-	// 2 m + k / 128 of a chunk (m < 16); ex [kCH][kSX] then ey [kCH][kSY]
+	// 2 m + k / 128 of a chunk (m < kCH / 2); ex [kCH][kSX] then ey [kCH][kSY]
 	static_assert(kSX == kSY && kSThr == 2 * (kSX + kSY), "staging map");
 	const int sr = threadIdx.x % (kSX + kSY), sa = threadIdx.x / (kSX + kSY);
 	const bool sx = sr < kSX;
 	const int sij = sx ? blockIdx.x * kSX + sr : blockIdx.y * kSY + sr - kSX;
-	const bool sin = sx ? sij < p.nx : sij < p.ny;
+	const bool sin = sx ? sij < p.nx : sij < hb;
 	const float2* ssrc = (sx ? txg : tyg) + (sin ? sij : 0);
 	const int sstr = sx ? p.nx : p.ny;
 	const int sdst = (sx ? sr : kCH * kSX + sr - kSX) + sa * kSX;
 	auto stage = [&](int c) {
 		float2* buf = smem + (c & 1) * kChunkF2 + sdst;
-		#pragma unroll 4
+		#pragma unroll
 		for (int m = 0; m < kCH / 2; m++) {
 			const int at = c * kCH + sa + 2 * m;
 			const bool ok = sin && at < natom;
@@ -192,9 +201,10 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 	#pragma unroll
 	for (int r = 0; r < kRW; r++) {
 		S[r][0] = S[r][1] = make_float2(0.f, 0.f);
-		pot[(2 * r) * kSThr] = pot[(2 * r + 1) * kSThr] = make_float2(0.f, 0.f);
+		#pragma unroll
+		for (int c = 0; c < 2; c++) pot[(2 * r + c) * kSThr] = pot[(16 + 2 * r + c) * kSThr] = make_float2(0.f, 0.f);
 	}
-	// pot += f_t(|q|) ap(q)^2 S_t(q); S = 0
+	// pot(q) += f_t S_t(q), pot(-q) += f_t conj(S_t(q)); S = 0
 	auto close_type = [&](int t) {
 		const float2* F = p.fq + (long long)t * p.nx * p.ny;
 		#pragma unroll
@@ -203,12 +213,17 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 			#pragma unroll
 			for (int c = 0; c < 2; c++) {
 				const int ix = ix0 + c;
-				const float2 f = (ix < p.nx && iy < p.ny) ? __ldg(F + (long long)iy * p.nx + ix) : make_float2(0.f, 0.f);
+				const float2 f = (ix < p.nx && iy < hb) ? __ldg(F + (long long)iy * p.nx + ix) : make_float2(0.f, 0.f);
 				const float fr = f.x, fi = f.y;
+				const float sxv = S[r][c].x, syv = S[r][c].y;
 				float2 pv = pot[(2 * r + c) * kSThr];
-				pv.x += fr * S[r][c].x - fi * S[r][c].y;
-				pv.y += fr * S[r][c].y + fi * S[r][c].x;
+				pv.x += fr * sxv - fi * syv;
+				pv.y += fr * syv + fi * sxv;
 				pot[(2 * r + c) * kSThr] = pv;
+				float2 pm = pot[(16 + 2 * r + c) * kSThr];
+				pm.x += fr * sxv - fi * (-syv);
+				pm.y += fr * (-syv) + fi * sxv;
+				pot[(16 + 2 * r + c) * kSThr] = pm;
 				S[r][c] = make_float2(0.f, 0.f);
 			}
 		}
@@ -255,10 +270,11 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 		__syncthreads();   // the buffer of chunk c is restaged for chunk c + 2
 	}
 	float2* out = p.out + (long long)g * p.gstride;
+	const int nyqx = (p.nx & 1) ? -1 : (p.nx >> 1);    // column without a sampled mirror
 	#pragma unroll
 	for (int r = 0; r < kRW; r++) {
 		const int iy = iy0 + r;
-		if (iy >= p.ny) break;
+		if (iy >= hb) break;
 		float2* o = out + (long long)iy * p.nx + ix0;
 		const float2 v0 = pot[(2 * r) * kSThr], v1 = pot[(2 * r + 1) * kSThr];
 		if (ix0 + 1 < p.nx && (p.nx & 1) == 0)
@@ -267,12 +283,46 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 			if (ix0 < p.nx) o[0] = v0;
 			if (ix0 + 1 < p.nx) o[1] = v1;
 		}
+		if (iy == 0) continue;                          // row 0 is its own mirror: summed in full
+		float2* om = out + (long long)(p.ny - iy) * p.nx;
+		#pragma unroll
+		for (int c = 0; c < 2; c++) {
+			const int ix = ix0 + c;
+			if (ix < p.nx && ix != nyqx) om[ix == 0 ? 0 : p.nx - ix] = pot[(16 + 2 * r + c) * kSThr];
+		}
 	}
+}
+
+// One thread per pixel without a sampled mirror: the Nyquist row ny / 2 (even
+// ny, all columns), then the Nyquist column nx / 2 (even nx) of the mirrored
+// rows ny - iy, 1 <= iy < ceil(ny / 2).
+__global__ void k_pgr_lines(const PgrArgs p, int nrow, int npts)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x, g = blockIdx.z;
+	if (k >= npts) return;
+	int ix, iy;
+	if (k < nrow) { ix = k; iy = p.ny >> 1; }
+	else { ix = p.nx >> 1; iy = p.ny - (1 + k - nrow); }
+	const float2* txg = p.tx + (long long)g * p.natom * p.nx + ix;
+	const float2* tyg = p.ty + (long long)g * p.natom * p.ny + iy;
+	float2 pot = make_float2(0.f, 0.f);
+	for (int t = 0; t < p.ntype; t++) {
+		float2 S = make_float2(0.f, 0.f);
+		for (int a = p.type_start[t]; a < p.type_start[t + 1]; a++) {
+			const float2 e = __ldg(txg + (long long)a * p.nx), w = __ldg(tyg + (long long)a * p.ny);
+			cmac(S, e.x, e.y, w.x, w.y);
+		}
+		const float2 f = __ldg(p.fq + ((long long)t * p.ny + iy) * p.nx + ix);
+		const float fr = f.x, fi = f.y;
+		pot.x += fr * S.x - fi * S.y;
+		pot.y += fr * S.y + fi * S.x;
+	}
+	p.out[(long long)g * p.gstride + (long long)iy * p.nx + ix] = pot;
 }
 
 cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s)
 {
-	constexpr int smem = (2 * kChunkF2 + 2 * kRW * kSThr) * (int)sizeof(float2);
+	constexpr int smem = (2 * kChunkF2 + 32 * kSThr) * (int)sizeof(float2);
 	// the dynamic shared-memory limit is raised once per device
 	static bool attr_set[64] = {};
 	int dev = 0;
@@ -284,9 +334,20 @@ cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s)
 		if (e != cudaSuccess) return e;
 		attr_set[dev] = true;
 	}
-	const dim3 grid((p.nx + kSX - 1) / kSX, (p.ny + kSY - 1) / kSY, p.ngr);
+	const int hb = (p.ny + 1) >> 1;
+	const dim3 grid((p.nx + kSX - 1) / kSX, (hb + kSY - 1) / kSY, p.ngr);
 	k_pgr_synth<<<grid, kSThr, smem, s>>>(p);
-	return cudaGetLastError();
+	if ((e = cudaGetLastError()) != cudaSuccess) return e;
+	// pixels without a sampled mirror: Nyquist row (even ny), Nyquist column
+	// of the mirrored rows (even nx)
+	const int nrow = (p.ny & 1) ? 0 : p.nx;
+	const int ncol = (p.nx & 1) ? 0 : hb - 1;
+	const int npts = nrow + ncol;
+	if (npts > 0) {
+		k_pgr_lines<<<dim3((npts + 127) / 128, 1, p.ngr), 128, 0, s>>>(p, nrow, npts);
+		e = cudaGetLastError();
+	}
+	return e;
 }
 
 // ---------------------------------------------------------------------------

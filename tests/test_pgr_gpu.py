@@ -57,6 +57,23 @@ def test_pgr_band_limit_switches(J, bwl_pot, bwl_pgr):
     assert np.abs(t[0] - o).max() < TOL_FP64
 
 
+@pytest.mark.parametrize("nx,ny", [(64, 96), (80, 120), (40, 80)])
+def test_pgr_grid_shapes(J, nx, ny):
+    """Non-square grids whose width and half height are not multiples of the
+    synthesis tile: the rows summed directly, their mirrors (ny - iy,
+    (nx - ix) mod nx) and the Nyquist row and column all against the FP64
+    oracle.  The shapes keep every pixel at least 1e-4 (relative) away from the
+    2/3 band-limit radius on this cell: on a pixel exactly at that radius (80 x
+    48, 96 x 48 here) the aperture's float comparison, which follows the
+    reference, and the oracle's double comparison may disagree."""
+    c = dict(PG.golden("g1"), nx=nx, ny=ny)
+    atoms, tb = _setup(J, c)
+    e, t = J.pgr_calculate(atoms, c["c"])
+    assert e == 0
+    site_of, base, _ = PG.sites(atoms, c["a"], c["b"], c["c"], tb, c["thermal"])
+    assert np.abs(t[0] - _oracle(c, atoms, base[site_of])).max() < TOL_FP64
+
+
 def test_pgr_qep_draws(J):
     """Every grating of a QEP batch is the grating of its own displaced sites."""
     c = PG.golden("g2")
