@@ -890,8 +890,10 @@ def measure_multifidelity(J, cfg, stream, d_pos, npos_step, rows, warmup, n_low=
     one on the same raster rows and the same 16 phonon configurations: plain =
     16 full-grid passes per position; chosen = 1 full-grid pass + 16 passes on a
     n_low^2 grid of the same specimen (control variate, coefficient 1), n_low
-    the coarsest supported grid whose band limit covers the 20-50 mrad detector
-    (192 at 300 kV on the 23.43 A cell: 54 mrad).  The chosen form takes
+    the coarsest grid among the candidates whose band limit covers the 20-50 mrad
+    detector (192 at 300 kV on the 23.43 A cell: 54 mrad; 180 would reach
+    50.4 mrad, but its 12 x 15 line plan runs 1.6x slower per point, so the
+    chosen form took 100.6 ms per raster row with it against 77.8 with 192).  The chosen form takes
     `group` raster rows per call, so that the coarse grid's launches carry
     group x 64 waves (its 192^2 waves are small); the plain form takes one row
     per call (64 waves of 512^2 already fill a launch).  Times per raster row

@@ -23,6 +23,7 @@ using P120 = Plan<10, 12, 16>;
 using P128a = Plan<8, 16, 16>;
 using P128b = Plan<16, 8, 16>;
 using P160 = Plan<10, 16, 16>;
+using P180 = Plan<12, 15, 16>;
 using P192 = Plan<12, 16, 16>;
 using P240 = Plan<15, 16, 16>;
 using P256a = Plan<16, 16, 16>;
@@ -55,7 +56,7 @@ template <class PL> cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 #define JMS_PLANS(X) \
 	X(16, P16, "4x16") X(24, P24, "4x6") X(32, P32, "4x8 pair") X(40, P40, "5x8") X(48, P48, "6x8") \
 	X(64, P64a, "8x8") X(64, P64b, "4x4x4") X(80, P80, "8x10") X(96, P96, "8x12") X(120, P120, "10x12") \
-	X(128, P128a, "8x16 pair") X(128, P128b, "16x8") X(160, P160, "10x16") X(192, P192, "12x16") \
+	X(128, P128a, "8x16 pair") X(128, P128b, "16x8") X(160, P160, "10x16") X(180, P180, "12x15") X(192, P192, "12x16") \
 	X(240, P240, "15x16") X(256, P256a, "16x16 c16") X(256, P256b, "16x16 c8") X(256, P256p, "16x16 c8 pipe") X(320, P320, "16x20") \
 	X(384, P384, "16x24") X(480, P480, "20x24") X(512, P512a, "16x32 pair c16") X(512, P512b, "8x8x8 c8") \
 	X(512, P512c, "16x32 pair c8") \
@@ -68,6 +69,6 @@ template <class PL> cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 // jms_pgr_ops_*.cu)
 #define JMS_DEFAULT_PLANS_0(X) \
 	X(16, P16) X(24, P24) X(32, P32) X(40, P40) X(48, P48) X(64, P64a) X(80, P80) X(96, P96) X(120, P120) \
-	X(128, P128a) X(160, P160) X(192, P192) X(240, P240) X(256, P256a)
+	X(128, P128a) X(160, P160) X(180, P180) X(192, P192) X(240, P240) X(256, P256a)
 #define JMS_DEFAULT_PLANS_1(X) X(320, P320) X(384, P384) X(480, P480) X(512, P512a) X(640, P640) X(720, P720)
 #define JMS_DEFAULT_PLANS_2(X) X(768, P768) X(960, P960) X(1024, P1024a) X(2048, P2048a)
