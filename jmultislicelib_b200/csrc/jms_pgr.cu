@@ -64,10 +64,10 @@ cudaError_t launch_pgr_sites(double2* pos, const double2* base, const double* ux
 //                S(-q) = conj(S(q)): tiles cover rows iy < ceil(ny / 2) and
 //                also write f_t conj(S_t) at the mirrored pixel
 //                (ny - iy, (nx - ix) mod nx);
-//   k_pgr_lines: the pixels without a sampled mirror, summed directly: the
-//                Nyquist row ny / 2 (even ny) and the Nyquist column nx / 2
-//                of the mirrored rows (even nx), where the grid samples -n/2
-//                and not its partner +n/2.
+//   k_pgr_lines: the pixels without a sampled mirror, summed directly from
+//                the same tables: the Nyquist row ny / 2 (even ny) and the
+//                Nyquist column nx / 2 of the mirrored rows (even nx), where
+//                the grid samples -n/2 and not its partner +n/2.
 // Every output sums its atoms in type order, then atom order, with two FMAs
 // per component and atom, and adds f_t S_t over the types in order.
 namespace {
@@ -293,31 +293,46 @@ __global__ void __launch_bounds__(kSThr, 2) k_pgr_synth(const PgrArgs p)
 	}
 }
 
-// One thread per pixel without a sampled mirror: the Nyquist row ny / 2 (even
-// ny, all columns), then the Nyquist column nx / 2 (even nx) of the mirrored
-// rows ny - iy, 1 <= iy < ceil(ny / 2).
-__global__ void k_pgr_lines(const PgrArgs p, int nrow, int npts)
+// The pixels without a sampled mirror: the Nyquist row ny / 2 (even ny, all
+// columns), then the Nyquist column nx / 2 (even nx) of the mirrored rows
+// ny - iy, 1 <= iy < ceil(ny / 2).  A CTA takes 32 consecutive pixels (one
+// per lane, so the table reads coalesce); its 8 warps share the atoms of each
+// type (warp w: atoms w, w + 8, ...), and warp 0 adds their partial sums in
+// warp order.
+constexpr int kLineWarps = 8;
+__global__ void __launch_bounds__(32 * kLineWarps) k_pgr_lines(const PgrArgs p, int nrow, int npts)
 {
-	const int k = blockIdx.x * blockDim.x + threadIdx.x, g = blockIdx.z;
-	if (k >= npts) return;
-	int ix, iy;
+	__shared__ float2 part[kLineWarps][32];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = blockIdx.z;
+	const int k = blockIdx.x * 32 + lane;
+	const bool live = k < npts;
+	int ix = 0, iy = 0;
 	if (k < nrow) { ix = k; iy = p.ny >> 1; }
-	else { ix = p.nx >> 1; iy = p.ny - (1 + k - nrow); }
+	else if (live) { ix = p.nx >> 1; iy = p.ny - (1 + k - nrow); }
 	const float2* txg = p.tx + (long long)g * p.natom * p.nx + ix;
 	const float2* tyg = p.ty + (long long)g * p.natom * p.ny + iy;
 	float2 pot = make_float2(0.f, 0.f);
 	for (int t = 0; t < p.ntype; t++) {
 		float2 S = make_float2(0.f, 0.f);
-		for (int a = p.type_start[t]; a < p.type_start[t + 1]; a++) {
-			const float2 e = __ldg(txg + (long long)a * p.nx), w = __ldg(tyg + (long long)a * p.ny);
-			cmac(S, e.x, e.y, w.x, w.y);
+		if (live)
+			for (int a = p.type_start[t] + w; a < p.type_start[t + 1]; a += kLineWarps) {
+				const float2 e = __ldg(txg + (long long)a * p.nx), v = __ldg(tyg + (long long)a * p.ny);
+				cmac(S, e.x, e.y, v.x, v.y);
+			}
+		part[w][lane] = S;
+		__syncthreads();
+		if (w == 0 && live) {
+			S = part[0][lane];
+			#pragma unroll
+			for (int q = 1; q < kLineWarps; q++) S = make_float2(S.x + part[q][lane].x, S.y + part[q][lane].y);
+			const float2 f = __ldg(p.fq + ((long long)t * p.ny + iy) * p.nx + ix);
+			const float fr = f.x, fi = f.y;
+			pot.x += fr * S.x - fi * S.y;
+			pot.y += fr * S.y + fi * S.x;
 		}
-		const float2 f = __ldg(p.fq + ((long long)t * p.ny + iy) * p.nx + ix);
-		const float fr = f.x, fi = f.y;
-		pot.x += fr * S.x - fi * S.y;
-		pot.y += fr * S.y + fi * S.x;
+		__syncthreads();
 	}
-	p.out[(long long)g * p.gstride + (long long)iy * p.nx + ix] = pot;
+	if (w == 0 && live) p.out[(long long)g * p.gstride + (long long)iy * p.nx + ix] = pot;
 }
 
 cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s)
@@ -344,7 +359,7 @@ cudaError_t launch_pgr_synth(const PgrArgs& p, cudaStream_t s)
 	const int ncol = (p.nx & 1) ? 0 : hb - 1;
 	const int npts = nrow + ncol;
 	if (npts > 0) {
-		k_pgr_lines<<<dim3((npts + 127) / 128, 1, p.ngr), 128, 0, s>>>(p, nrow, npts);
+		k_pgr_lines<<<dim3((npts + 31) / 32, 1, p.ngr), 32 * kLineWarps, 0, s>>>(p, nrow, npts);
 		e = cudaGetLastError();
 	}
 	return e;
