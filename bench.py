@@ -776,7 +776,7 @@ def run_qep(args):
     torch.cuda.set_device(0)
     cfg = dict(S.SCAN_512)
     J = jb.JMS()
-    stream = torch.cuda.Stream()
+    stream = torch.cuda.Stream(priority=-1)        # scans; grating generation runs on a lower-priority stream
     J.set_stream(stream.cuda_stream)
     J.L.JMS_SetScanBatch(args.batch)
     nobj, nst = cfg["nobj"], cfg["nslice_types"]
@@ -795,11 +795,13 @@ def run_qep(args):
     abrr = np.zeros(48, np.float32)
     abrr[10] = cfg["cs"]
     probe = J.calc_probe(cfg["alpha"], abrr=abrr)
-    # the grating store holds every configuration of a step: structure slice s
-    # has count[s] x nconf variants, variant k * count[s] + r being the r-th
-    # object slice of type s in configuration k
-    nconf = cfg["nvar"]
-    assert J.setup(2, [c * nconf for c in count], objslc, [0] * nst, cfg["ndetper"], len(dets), 1) == [0, 0, 0, 0]
+    # the grating store holds every configuration of a step, twice (two halves
+    # that alternate between steps): structure slice s has count[s] x nconf x 2
+    # variants, variant (h nconf + k) count[s] + r being the r-th object slice
+    # of type s in configuration k of half h
+    nconf, nhalf = cfg["nvar"], 2
+    assert J.setup(2, [c * nconf * nhalf for c in count], objslc, [0] * nst, cfg["ndetper"], len(dets),
+                   1) == [0, 0, 0, 0]
     assert J.set_propagator(2, 0, pro) == 0
     for i, (d, m) in enumerate(dets):
         assert J.set_detector(2, i, d, m) == 0
@@ -819,41 +821,80 @@ def run_qep(args):
     ir, ic = C.c_int(0), C.c_int(0)
     assert J.L.JMS_Autotune(min(args.batch, npos * nconf), 20, None, None, C.byref(ir), C.byref(ic)) == 0
     cnt = np.asarray(count, np.int32)[objslc]
-    vs = np.ascontiguousarray(np.stack([k * cnt + rank for k in range(nconf)]), np.int32)
-    vsp = vs.ctypes.data_as(C.POINTER(C.c_int))
+    vs = [np.ascontiguousarray(np.stack([(h * nconf + k) * cnt + rank for k in range(nconf)]), np.int32)
+          for h in range(nhalf)]
+    gstream = torch.cuda.Stream(priority=0)        # generation; the scan stream has the higher priority
 
-    def step(k):
-        # nconf fresh configurations (count[s] new gratings per slice type each),
-        # then one scan over all of them (their waves share the launches)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
+    def generate(k):
+        # nconf fresh configurations of step k (count[s] new gratings per slice type each) into half k % 2
+        h = k % nhalf
         for p in range(nconf):
             for s_ in range(nst):
                 e, _ = J.pgr_calculate(layers[s_], S.DZ_SLICE, ngr=count[s_], seed=(1000 * k + p) * 16 + s_,
-                                       islc=s_, ivar0=p * count[s_], want=False)
+                                       islc=s_, ivar0=(h * nconf + p) * count[s_], want=False)
                 assert e == 0, e
-        ev1.record(stream)
-        e = J.L.JMS_ScanGPUDevice(npos, d_pos.data_ptr(), 0.0, nconf, vsp, d_int.data_ptr(), None, 0)
+
+    def scan(k):
+        # one scan over the nconf configurations of step k (their waves share the launches)
+        v = vs[k % nhalf]
+        e = J.L.JMS_ScanGPUDevice(npos, d_pos.data_ptr(), 0.0, nconf, v.ctypes.data_as(C.POINTER(C.c_int)),
+                                  d_int.data_ptr(), None, 0)
         assert e == 0, e
-        ev2 = torch.cuda.Event(enable_timing=True)
-        ev2.record(stream)
-        return [(ev0, ev1, ev2)]
+
+    def serial(k0, n, evs):
+        # generation and scan of each step in turn on the scan stream
+        J.pgr_set_stream(0)
+        for k in range(k0, k0 + n):
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            generate(k)
+            e1.record(stream)
+            scan(k)
+            e2.record(stream)
+            evs.append((e0, e1, e2))
+
+    def overlapped(k0, n):
+        # generation of step k + 1 (generator stream) runs during the scan of
+        # step k (scan stream): a scan waits for its gratings, a generation
+        # for the scan that last read its half
+        J.pgr_set_stream(gstream.cuda_stream)
+        gstream.wait_stream(stream)
+        ev_gen, ev_scan = {}, {}
+        with torch.cuda.stream(gstream):
+            generate(k0)
+        ev_gen[k0] = torch.cuda.Event()
+        ev_gen[k0].record(gstream)
+        for k in range(k0, k0 + n):
+            if k + 1 < k0 + n:
+                if k - 1 in ev_scan:
+                    gstream.wait_event(ev_scan[k - 1])
+                with torch.cuda.stream(gstream):
+                    generate(k + 1)
+                ev_gen[k + 1] = torch.cuda.Event()
+                ev_gen[k + 1].record(gstream)
+            stream.wait_event(ev_gen[k])
+            scan(k)
+            ev_scan[k] = torch.cuda.Event()
+            ev_scan[k].record(stream)
+        J.pgr_set_stream(0)
+
+    def timed(fn, k0, *extra):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                fn(k0, args.steps, *extra)
+                ev1.record(stream)
+            torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1), clk.summary()
 
     with torch.cuda.stream(stream):
-        for k in range(args.warmup):
-            step(k)
+        serial(0, args.warmup, [])
+        overlapped(args.warmup, args.warmup)
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    gen_ms = 0.0
-    with ClockSampler(0) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            all_ev = []
-            for k in range(args.steps):
-                all_ev += step(args.warmup + k)
-            ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    all_ev = []
+    ms_serial, _ = timed(serial, 2 * args.warmup, all_ev)
+    ms, clocks = timed(overlapped, 2 * args.warmup + args.steps)
     gen_ms = sum(a.elapsed_time(b) for a, b, _ in all_ev)
     scan_ms = sum(b.elapsed_time(c) for _, b, c in all_ev)
     steps_per = npos * cfg["nvar"] * nobj
@@ -863,10 +904,15 @@ def run_qep(args):
             "config": {"workload": "STEM scan row: 64 positions x 16 phonon passes x 200 slices, 512x512; every "
                                    "pass a new QEP configuration: 200 gratings generated on the device "
                                    "(sigma 0.08 A, Gaussian form factors, 2/3 band limit); the 16 configurations "
-                                   "of a step (3,200 gratings) are generated first, then scanned together",
+                                   "of a step (3,200 gratings) are generated into one half of a double grating "
+                                   "store while the previous step's half is scanned (generator stream of its own, "
+                                   "JMS_PgrSetStream; the scan stream has the higher priority)",
                        "batch_waves": min(args.batch, 64 * nconf)},
-            "grating_generation_share": gen_ms / ms,
-            "scan_only_steps_per_s": args.steps * steps_per / (scan_ms / 1e3), "clocks": clk.summary()}
+            "serial": {"value": args.steps * steps_per / (ms_serial / 1e3), "ms_per_step": ms_serial / args.steps,
+                       "grating_generation_share": gen_ms / ms_serial,
+                       "scan_only_steps_per_s": args.steps * steps_per / (scan_ms / 1e3),
+                       "note": "generation, then scan, on one stream"},
+            "clocks": clocks}
     print(json.dumps(line))
     return 0
 

@@ -360,6 +360,14 @@ int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int b
  * sample k at q = k * sk [1/nm] (the table CAtomType::CopyFormFactors returns,
  * src/Atoms.h:122-125), and Biso [nm^2] per type (QEP amplitudes; may be NULL). */
 int JMS_PgrSetFormFactors(int ntype, int nk, float sk, const float* ff, const float* biso);
+/* Stream of the generator's kernels; NULL (the default) runs them on the
+ * current context's stream.  With a stream of its own, the generation of one
+ * set of gratings can overlap the scans of the context's stream.  The caller
+ * orders the two with events: a scan waits for the generation of the gratings
+ * it reads, and a generation into grating variants waits for the scans still
+ * reading them.  No reference counterpart (CJEElaSca's GPU path runs on the
+ * default stream); returns 0. */
+int JMS_PgrSetStream(void* stream);
 /* ngr phase gratings of one structure slice: atoms [natom][5] = fractional
  * x, y, z in the cell, occupancy, type index; cz = slice thickness [nm].
  * Atoms closer than 0.05 nm share a site (CStructure::SetAtomSites,

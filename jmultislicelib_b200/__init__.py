@@ -98,6 +98,7 @@ SIGNATURES = {
     "JMS_SliLoadSlice": ([C.c_char_p, _i], _i),
     "JMS_PgrSetup": ([_i, _i, _f, _f, _f, _i, _i, _i], _i),
     "JMS_PgrSetFormFactors": ([_i, _i, _f, _fp, _fp], _i),
+    "JMS_PgrSetStream": ([_p], _i),
     "JMS_PgrCalculate": ([_i, _fp, _f, _i, C.c_ulonglong, _i, _i, _fp], _i),
     "JMS_ReadoutDetectorsNoAlloc": ([_p, _i, _p, _p], _i),
     "JMS_Autotune": ([_i, _i, _fp, _fp, _ip, _ip], _i),
@@ -303,6 +304,10 @@ class JMS:
         ff = _c64(ff)
         bi = None if biso is None else np.ascontiguousarray(biso, np.float32)
         return self.L.JMS_PgrSetFormFactors(ff.shape[0], ff.shape[1], sk, _fptr(ff), None if bi is None else _fptr(bi))
+
+    def pgr_set_stream(self, stream_ptr):
+        """Stream of the generator's kernels (0 / None: the context's stream)."""
+        return self.L.JMS_PgrSetStream(C.c_void_p(stream_ptr or None))
 
     def pgr_calculate(self, atoms, cz, ngr=1, seed=0, islc=-1, ivar0=0, want=True):
         """atoms [natom, 5]: fractional x, y, z, occupancy, type.  Returns

@@ -50,6 +50,7 @@ static jms::PgrGen& G()
 }
 
 static int g_debug = 0;
+static cudaStream_t g_pgr_stream = nullptr;   // generator stream (JMS_PgrSetStream); nullptr: the context's
 
 extern "C" {
 
@@ -428,6 +429,11 @@ int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int b
 }
 int JMS_PgrSetFormFactors(int ntype, int nk, float sk, const float* ff, const float* biso)
 { return G().SetFormFactors(ntype, nk, sk, ff, biso); }
+int JMS_PgrSetStream(void* stream)
+{
+	g_pgr_stream = (cudaStream_t)stream;
+	return 0;
+}
 int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned long long seed, int islc, int ivar0,
 	float* pgr)
 {
@@ -437,7 +443,7 @@ int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned 
 		dst = J().GratingSlot(islc, ivar0, ngr, &npgx, &npgy);
 		if (dst == nullptr || npgx != G().nx() || npgy != G().ny()) return 9;
 	}
-	cudaStream_t s = J().Stream();
+	cudaStream_t s = g_pgr_stream ? g_pgr_stream : J().Stream();
 	G().SetStream(s);
 	int e = G().Calculate(natom, atoms, cz, ngr, seed, dst, pgr);
 	// before InitCore the context has no stream of its own yet, and the one it

@@ -166,6 +166,58 @@ def test_pgr_into_multislice_setup(J):
     J.cleanup()
 
 
+def test_pgr_own_stream(J):
+    """Gratings generated on a stream of the generator's own (JMS_PgrSetStream),
+    ordered before the scan by an event, give the scan on the context's stream
+    the same result as gratings generated on that stream itself."""
+    import torch
+
+    c = PG.golden("g0")
+    nx, ny = c["nx"], c["ny"]
+    atoms, tb = _setup(J, c, thermal=2)
+    cs, gs = torch.cuda.Stream(), torch.cuda.Stream()
+    objslc = np.arange(12) % 2
+    pos = np.random.default_rng(3).uniform(0, c["a"], (5, 2)).astype(np.float32)
+    varseq = np.stack([objslc * 0 + (k % 3) for k in range(2)]).astype(np.int32)
+
+    def run(own):
+        J.cleanup()
+        J.set_stream(cs.cuda_stream)
+        J.set_high_tension(300.0)
+        J.set_grid(nx, ny, c["a"], c["b"], c["c"])
+        pro = J.calc_propagator(c["c"], 0.0, 0.0, 1)
+        dets = [J.calc_ring_detector(b0, b1) for (b0, b1) in ((0, 10), (20, 50), (80, 200))]
+        assert J.setup(GPU, [3, 3], objslc, [0, 0], 4, 3, G.INT) == [0, 0, 0, 0]
+        assert J.set_propagator(GPU, 0, pro) == 0
+        for i, (d, m) in enumerate(dets):
+            assert J.set_detector(GPU, i, d, m) == 0
+        assert J.init_core(GPU) == 0
+        assert J.set_incident_wave(GPU, J.calc_probe(25.0)) == 0
+        torch.cuda.synchronize()
+        if own:
+            J.pgr_set_stream(gs.cuda_stream)
+        for s in range(2):
+            e, _ = J.pgr_calculate(atoms, c["c"], ngr=3, seed=100 + s, islc=s, ivar0=0, want=False)
+            assert e == 0
+        if own:
+            ev = torch.cuda.Event()
+            ev.record(gs)
+            cs.wait_event(ev)
+            J.pgr_set_stream(0)
+        e, out, _ = J.scan(pos, 2, varseq=varseq)
+        assert e == 0
+        return out
+
+    try:
+        ref = run(False)
+        np.testing.assert_array_equal(run(True), ref)
+        assert np.abs(ref).max() > 0
+    finally:
+        J.pgr_set_stream(0)
+        J.cleanup()
+        J.set_stream(0)
+
+
 def test_pgr_errors(J):
     c = PG.golden("g0")
     assert J.pgr_setup(100, 64, c["a"], c["b"], 300.0) == 8          # no line plan for 100
