@@ -364,23 +364,26 @@ __device__ __forceinline__ void block_store_partials(const float (&acc)[kMaxDet]
 	__syncthreads();
 }
 
-// Fourier-space readout of one element psi(ky = y, kx) of wave b
-// (ReadoutDifDet_d, src/JMultiSlice.cpp:4277-4359).
-__device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y, int kx, float2 v,
-	float (&acc)[kMaxDet])
+// Scrambled pixel index at which psi(ky = y, kx) is read out, after the
+// integer-pixel diffraction descan (DescanDifN, src/JMultiSlice.cpp:2184-2273:
+// psi(kx, ky) is read out at pixel (kx - dnx, ky - dny), periodic)
+__device__ __forceinline__ void readout_pixel(const PassArgs& p, int& y, int& kx)
 {
-	const long long N = (long long)p.nx * p.ny;
 	if (p.descan_x | p.descan_y) {
-		// integer-pixel diffraction descan (DescanDifN, src/JMultiSlice.cpp:2184-2273):
-		// psi(kx, ky) is read out at pixel (kx - dnx, ky - dny), periodic
 		kx -= p.descan_x; kx %= p.nx; if (kx < 0) kx += p.nx;
 		y -= p.descan_y; y %= p.ny; if (y < 0) y += p.ny;
 	}
-	const long long idx = (long long)y * p.nx + kx;
+}
+
+// Fourier-space readout of one element psi(ky = y, kx) of wave b
+// (ReadoutDifDet_d, src/JMultiSlice.cpp:4277-4359) except the integrating
+// detectors: diffraction and wave channels, binned pattern.
+__device__ __forceinline__ void readout_fourier_channels(const PassArgs& p, int b, int y, int kx, float2 v)
+{
+	const long long N = (long long)p.nx * p.ny;
+	readout_pixel(p, y, kx);
+	const int idx = y * p.nx + kx;                    // nx * ny < 2^31
 	const float pw = cnorm(v);
-	#pragma unroll
-	for (int d = 0; d < kMaxDet; d++)
-		if (d < p.ndet) acc[d] = fmaf(pw, __ldg(p.det + d * N + idx), acc[d]);
 	const long long c = (long long)b * p.chan_wstride + (long long)p.plane * N + idx;
 	if (p.dif) p.dif[c] += p.weight * pw;
 	if (p.dif_avg) p.dif_avg[c] += p.weight * pw;
@@ -396,6 +399,43 @@ __device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y,
 		if (bx < p.nbx && by < p.nby)
 			atomicAdd(p.bin_out + ((long long)bp * p.nby + by) * p.nbx + bx, p.weight * pw);
 	}
+}
+
+// Fourier-space readout of one element psi(ky = y, kx) of wave b
+// (ReadoutDifDet_d, src/JMultiSlice.cpp:4277-4359): integrating detectors
+// into acc, then the channels.
+__device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y, int kx, float2 v,
+	float (&acc)[kMaxDet])
+{
+	int yd = y, kxd = kx;
+	readout_pixel(p, yd, kxd);
+	const int idx = yd * p.nx + kxd;                  // nx * ny < 2^31
+	const float pw = cnorm(v);
+	const float* det = p.det + idx;
+	const int N = p.nx * p.ny;
+	#pragma unroll
+	for (int d = 0; d < kMaxDet; d++)
+		if (d < p.ndet) acc[d] = fmaf(pw, __ldg(det + d * N), acc[d]);
+	readout_fourier_channels(p, b, y, kx, v);
+}
+
+// Sum of s over the CTA, stored as the partial of detector d (the warp sums
+// added in warp order, as block_store_partials does).
+template <int NT>
+__device__ __forceinline__ void block_store_partial(float s, const PassArgs& p, int b, int d)
+{
+	__shared__ float red1[NT / 32];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	s = warp_sum(s);
+	if (lane == 0) red1[warp] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		float t = 0.f;
+		#pragma unroll
+		for (int w = 0; w < NT / 32; w++) t += red1[w];
+		p.partial[(((long long)b * p.ndetslc + p.plane) * p.ndet + d) * p.nblk + blockIdx.x] = t;
+	}
+	__syncthreads();
 }
 
 // Real-space readout of psi(y, x) of wave b (ReadoutImgDet_d, src/JMultiSlice.cpp:4392-4459).
@@ -487,8 +527,18 @@ k_entry_rows(const PassArgs p)
 // Row pass: FT_x -> x P -> Fourier readout (plane) -> IFT_x.  READ selects
 // the variant with the readout code (used at readout planes only), so the
 // steps without readout do not carry its registers.
+// Resident CTAs asked of the readout variant: for plans of at most 16 values
+// a thread (whose plain pass takes 64 registers) the plain pass's count, so
+// the readout code spills a few bytes instead of halving the occupancy;
+// larger plans are held to about 112 registers.
+template <class PL>
+__host__ __device__ constexpr int read_min_blocks()
+{
+	return 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) > 0
+		? 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) : 1;
+}
 template <class PL, bool READ>
-__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, READ ? read_min_blocks<PL>() : 1)
 k_row_pass(const PassArgs p)
 {
 	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
@@ -514,24 +564,42 @@ k_row_pass(const PassArgs p)
 		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
 	PL::template to_mid<false, T>(v, sm, p.twx, tid);
-	float acc[kMaxDet];
-	#pragma unroll
-	for (int d = 0; d < kMaxDet; d++) acc[d] = 0.f;
 	{
 		int pos;
 		T::template role<PL::TMID>(tid, line, pos);
-		if (line < nval && pos < PL::TMID) {
-			const int y = row0 + line;
+		const bool mid_live = line < nval && pos < PL::TMID;
+		const int y = row0 + line;
+		if (mid_live) {
 			const float2* P = p.mul + (long long)y * N;
 			#pragma unroll
-			for (int e = 0; e < PL::EMID; e++) {
-				const int kx = PL::mid(pos, e);
-				v[e] = cmul(v[e], __ldg(P + kx));
-				if (READ) readout_fourier(p, b, y, kx, v[e], acc);
+			for (int e = 0; e < PL::EMID; e++) v[e] = cmul(v[e], __ldg(P + PL::mid(pos, e)));
+		}
+		if (READ) {
+			// channels in a loop of their own (uniform test), so their
+			// registers do not add to those of the propagator loads
+			const bool chan = p.dif || p.dif_avg || p.wff || p.wff_avg || (p.bin_out && p.plane == p.bin_plane);
+			if (chan && mid_live) {
+				#pragma unroll
+				for (int e = 0; e < PL::EMID; e++) readout_fourier_channels(p, b, y, PL::mid(pos, e), v[e]);
+			}
+			// integrating detectors one at a time (a rolled loop): unrolled
+			// over the detectors, the compiler kept every element's detector
+			// loads in flight (128 registers, half the plain pass's occupancy)
+			for (int d = 0; d < p.ndet; d++) {
+				float s = 0.f;
+				if (mid_live) {
+					const float* det = p.det + (long long)d * p.nx * p.ny;   // detector d: [ny][nx]
+					#pragma unroll
+					for (int e = 0; e < PL::EMID; e++) {
+						int yd = y, kx = PL::mid(pos, e);
+						readout_pixel(p, yd, kx);
+						s = fmaf(cnorm(v[e]), __ldg(det + yd * p.nx + kx), s);
+					}
+				}
+				block_store_partial<NT>(s, p, b, d);
 			}
 		}
 	}
-	if (READ && p.ndet > 0) block_store_partials<NT>(acc, p, b);
 	if (!p.store) return;
 	PL::template from_mid<true, T>(v, sm, p.twx, tid);
 	if (live) {
