@@ -525,21 +525,11 @@ k_entry_rows(const PassArgs p)
 }
 
 // Row pass: FT_x -> x P -> Fourier readout (plane) -> IFT_x.  READ selects
-// the variant with the readout code (used at readout planes only), so the
-// steps without readout do not carry its registers.
-// Resident CTAs asked of the readout variant: for plans of at most 16 values
-// a thread (whose plain pass takes 64 registers) the plain pass's count, so
-// the readout code spills a few bytes instead of halving the occupancy;
-// larger plans are held to about 112 registers.
-template <class PL>
-__host__ __device__ constexpr int read_min_blocks()
-{
-	return 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) > 0
-		? 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) : 1;
-}
+// the variant with the readout code (used at readout planes only, as the
+// kernel k_row_pass_read with launch bounds of its own), so the steps without
+// readout do not carry its registers.
 template <class PL, bool READ>
-__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, READ ? read_min_blocks<PL>() : 1)
-k_row_pass(const PassArgs p)
+__device__ __forceinline__ void row_pass_body(const PassArgs& p)
 {
 	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
 	using T = RowTile<L>;
@@ -607,6 +597,30 @@ k_row_pass(const PassArgs p)
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) dst[j + PL::B * m] = v[m];
 	}
+}
+
+// Resident CTAs asked of the readout kernel: for plans of at most 16 values
+// a thread (whose plain pass takes 64 registers) the plain pass's count, so
+// the readout code spills a few bytes instead of halving the occupancy;
+// larger plans are held to about 112 registers.
+template <class PL>
+__host__ __device__ constexpr int read_min_blocks()
+{
+	return 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) > 0
+		? 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) : 1;
+}
+// plain row pass (READ = false); the readout planes use k_row_pass_read
+template <class PL, bool READ>
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
+k_row_pass(const PassArgs p)
+{
+	row_pass_body<PL, READ>(p);
+}
+template <class PL>
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, read_min_blocks<PL>())
+k_row_pass_read(const PassArgs p)
+{
+	row_pass_body<PL, true>(p);
 }
 
 // Column pass: IFT_y -> real-space readout (plane) -> x t -> FT_y.
@@ -964,7 +978,7 @@ cudaError_t launch_row_t(const PassArgs& p, cudaStream_t s)
 	constexpr int L = row_lines<PL>();
 	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
 	const dim3 grid((p.ny + L - 1) / L, p.nwave);
-	if (p.plane >= 0) return launch_k(k_row_pass<PL, true>, grid, L * PL::TMAX, smem, p, s);
+	if (p.plane >= 0) return launch_k(k_row_pass_read<PL>, grid, L * PL::TMAX, smem, p, s);
 	if constexpr (PL::PIPE) {
 		if (p.store) {
 			// live row blocks: [0, split) and [split + skip, nrb)
