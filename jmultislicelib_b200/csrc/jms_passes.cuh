@@ -455,8 +455,9 @@ __device__ __forceinline__ void readout_real(const PassArgs& p, int b, int y, in
 // reduced mod 1 before the FP32 sincos (large k.dx phases keep full accuracy).
 __device__ __forceinline__ float2 offset_factor(const double* sh, int i, int j, int nx, int ny, float cp)
 {
-	const int fi = (i + (nx >> 1)) % nx - (nx >> 1);
-	const int fj = (j + (ny >> 1)) % ny - (ny >> 1);
+	// signed frequency index (i + n/2) mod n - n/2 of bin i < n, without a division
+	const int fi = i < nx - (nx >> 1) ? i : i - nx;
+	const int fj = j < ny - (ny >> 1) ? j : j - ny;
 	const double di = (double)fi, dj = (double)fj;
 	double t = di * sh[0] + dj * sh[1] + di * di * sh[2] + dj * dj * sh[3];
 	t -= floor(t);
@@ -499,12 +500,17 @@ k_entry_rows(const PassArgs p)
 			const int kx = j + PL::B * m;
 			float2 a;
 			if (p.shift) {
-				int sx = kx - p.ibtx, sy = y - p.ibty;
-				sx %= N; if (sx < 0) sx += N;
-				sy %= p.ny; if (sy < 0) sy += p.ny;
+				int sx = kx, sy = y;
+				if (p.ibtx | p.ibty) {   // beam tilt: a periodic shift of the incident wave (uniform branch)
+					sx -= p.ibtx; sx %= N; if (sx < 0) sx += N;
+					sy -= p.ibty; sy %= p.ny; if (sy < 0) sy += p.ny;
+				}
 				a = __ldg(p.wav0 + (long long)sy * N + sx);
-				const float cp = p.cppl ? __ldg(p.cppl + (long long)y * N + kx) : 0.f;
-				a = cmul(a, offset_factor(p.shift + 4 * b, kx, y, N, p.ny, cp));
+				// the offset phase only where the probe is nonzero (inside its aperture)
+				if (a.x != 0.f || a.y != 0.f) {
+					const float cp = p.cppl ? __ldg(p.cppl + (long long)y * N + kx) : 0.f;
+					a = cmul(a, offset_factor(p.shift + 4 * b, kx, y, N, p.ny, cp));
+				}
 			}
 			else {
 				a = p.wav0 ? __ldg(p.wav0 + (long long)y * N + kx) : W[(long long)y * N + kx];
