@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT}/include"]
-SOURCES = ["jms_kernels.cu", "jms_host.cpp", "jms_generators.cpp", "jms_capi.cpp", "jms_noalloc.cu", "jms_pgr.cu",
+SOURCES = ["jms_kernels.cu", "jms_host.cpp", "jms_generators.cpp", "jms_capi.cpp", "jms_class.cpp", "jms_noalloc.cu", "jms_pgr.cu",
            "jms_pgr_host.cpp", "jms_sli.cpp", "jms_nn.cu", "jms_tc.cu"] + [f"jms_inst_{k}.cu" for k in range(10)] + [f"jms_pgr_ops_{k}.cu" for k in range(3)]
 
 
@@ -34,7 +34,8 @@ def _newer(target: str, deps: list[str]) -> bool:
 
 def _headers() -> list[str]:
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    return hs + [os.path.join(ROOT, "include", "jms_b200.h")]
+    inc = os.path.join(ROOT, "include")
+    return hs + [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
 
 
 def _compile(src: str, verbose: bool) -> str:

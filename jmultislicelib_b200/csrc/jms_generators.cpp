@@ -32,13 +32,18 @@ static constexpr double kPI = 3.1415926535897932384626433832795;
 static constexpr double kTPI = 6.283185307179586476925286766559;
 static constexpr double kRelAperture = 0.666666666666667; // band limit (fraction of Nyquist)
 
+float wavelength_nm(float ht)
+{
+	// lambda [nm] = h c / e * 1e6 [nm keV] / sqrt(E (E + 2 m0 c^2)), E in keV
+	const double two_e0_kev = 2. * kME0 * kC0 * kC0 / kQEL / 1000.;
+	return (float)(kC0 * kHPL / kQEL * 1.0E+6 / std::sqrt(ht * (ht + two_e0_kev)));
+}
+
 float JmsB200::SetHighTension(float ht)
 {
 	const float old = ht_;
 	ht_ = ht;
-	// lambda [nm] = h c / e * 1e6 [nm keV] / sqrt(E (E + 2 m0 c^2)), E in keV
-	const double two_e0_kev = 2. * kME0 * kC0 * kC0 / kQEL / 1000.;
-	wl_ = (float)(kC0 * kHPL / kQEL * 1.0E+6 / std::sqrt(ht * (ht + two_e0_kev)));
+	wl_ = wavelength_nm(ht);
 	return old;
 }
 

@@ -50,8 +50,7 @@ int tuned_plan(int n, int axis)
 
 JmsB200::JmsB200()
 {
-	urng_.seed((unsigned)std::time(nullptr)); // CRng default: time-based seed
-	cudaGetDevice(&device_);
+	cudaGetDevice(&device_);   // own_rng_ is seeded from the clock, as CRng is
 }
 
 JmsB200::~JmsB200()
@@ -123,12 +122,7 @@ float JmsB200::GetSliceThickness(int islc) const
 // ---------------------------------------------------------------------------
 void JmsB200::SeedRngEx(int nseed)
 {
-	urng_.seed(nseed == 0 ? (unsigned)std::time(nullptr) : (unsigned)nseed);
-}
-
-double JmsB200::unirand(double a, double b)
-{
-	return a + ((double)uni_(urng_) / (double)((unsigned long)0x7FFFFFFF)) * (b - a);
+	rng_->seed(nseed);   // 0: seed from the clock
 }
 
 void JmsB200::SetPlasmonMC(bool use, float q_e, float q_c, float mfp, unsigned int nexmax)
@@ -149,8 +143,7 @@ int JmsB200::plasmon_step(float dt, int* di, int* dj)
 	// the wave moves by the change of round(q_total * a) pixels
 	*di = *dj = 0;
 	if (pl_mfp_ <= 0.f || pl_qe_ <= 0.f || pl_qc_ < pl_qe_) return 0;
-	std::poisson_distribution<int> pd((double)(dt / pl_mfp_));
-	const unsigned int n = std::min((unsigned int)pd(urng_), pl_nmax_ - pl_nex_);
+	const unsigned int n = std::min((unsigned int)rng_->poisrand((double)(dt / pl_mfp_)), pl_nmax_ - pl_nex_);
 	if (n == 0) return 0;
 	const float qe2 = pl_qe_ * pl_qe_, qc2 = pl_qc_ * pl_qc_;
 	float qx = 0.f, qy = 0.f;

@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <random>
+
+#include "../../include/rng.h"
 #include <string>
 #include <vector>
 
@@ -28,6 +30,9 @@ enum : int {
 	DET_INTEGRATED = 1, DET_IMAGE = 2, DET_DIFFRACTION = 4, DET_WAVEREAL = 8, DET_WAVEFOURIER = 16,
 	DET_IMAGE_AVG = 32, DET_DIFFR_AVG = 64, DET_WAVER_AVG = 128, DET_WAVEF_AVG = 256,
 };
+
+// electron wavelength [nm] at the kinetic energy ht [keV] (src/JMultiSlice.cpp:372-378)
+float wavelength_nm(float ht);
 
 // public probe parameters of CJProbeParams (src/JProbeGen.h:60-94)
 struct ProbeParams {
@@ -94,8 +99,11 @@ public:
 	int GetUnscrambleHash(unsigned int* phash) const;
 	int SetGPUPgrLoading(int npgrload);
 
-	// ---- RNG (src/rng.cpp:30-74 semantics)
+	// ---- RNG (src/rng.cpp:30-74 semantics): the context's own generator, or
+	// a caller's (CJMultiSlice::SetRng, src/JMultiSlice.cpp:347-370)
 	void SeedRngEx(int nseed);
+	void SetRng(CRng* prng) { rng_ = prng ? prng : &own_rng_; }
+	CRng* GetRng() { return rng_; }
 	int GetRandomVariantSequence(int* out);
 
 	// ---- calculation
@@ -201,10 +209,10 @@ private:
 	// everywhere (band limit); k1 = ny - 1 when every row has a nonzero value
 	std::vector<int> pro_k1_, pro_k2_;
 	std::vector<float> slcthick_;
-	// rng (CRng: std::mt19937, uniform ints 0..0x7FFFFFFF)
-	std::mt19937 urng_;
-	std::uniform_int_distribution<int> uni_{0, 0x7FFFFFFF};
-	double unirand(double a, double b);
+	// random numbers of the variant draws and plasmon paths
+	CRng own_rng_;
+	CRng* rng_ = &own_rng_;
+	double unirand(double a, double b) { return rng_->unirand(a, b); }
 	// device
 	int device_ = 0;
 	cudaStream_t stream_ = nullptr;

@@ -77,10 +77,17 @@ def projected_potential(nx, ny, a, b, atoms, amp, wid):
 
 
 def make_specimen(nx: int, ny: int, ncell_x: int, ncell_y: int, nslice_types: int, nvar: int, seed: int,
-                  kv: float = 300.0, sigma_disp: float = 0.008, keep_potential: bool = False) -> Specimen:
+                  kv: float = 300.0, sigma_disp: float = 0.008, keep_potential: bool = False,
+                  amp_scale: float = 1.0, wid_scale: float = 1.0) -> Specimen:
     """Specimen with nslice_types slice types (alternating A+O / B+2O layers,
-    each with its own phonon draws) and nvar frozen-phonon variants per type."""
+    each with its own phonon draws) and nvar frozen-phonon variants per type.
+    amp_scale and wid_scale multiply every atom's potential amplitudes and
+    widths (1, 1: the workload's weak-phase cell; larger amplitudes and
+    narrower atoms give a strongly scattering cell with the same geometry and
+    phonon draws)."""
     amp, wid = atom_params(seed)
+    amp = amp * amp_scale
+    wid = wid * wid_scale
     rng = np.random.default_rng(seed + 1)
     a, b = ncell_x * A_CELL, ncell_y * A_CELL
     sig = interaction_constant(kv)

@@ -32,11 +32,13 @@ _ip = C.POINTER(C.c_int)
 _lib = None
 
 
-def build(refsrc: str = "/root/reference/src") -> bool:
-    """Build the reference library when its sources are present."""
-    if not os.path.isdir(refsrc):
+def build(refroot: str | None = None) -> bool:
+    """Build the reference library when the reference project is present
+    (refroot, default: the JMS_REFERENCE environment variable)."""
+    refroot = refroot or os.environ.get("JMS_REFERENCE", "")
+    if not refroot or not os.path.isdir(os.path.join(refroot, "src")):
         return os.path.exists(LIB_PATH)
-    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFSRC={refsrc}", "-j8"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"JMS_REFERENCE={refroot}", "-j8"], check=True)
     return os.path.exists(LIB_PATH)
 
 
@@ -85,6 +87,7 @@ def lib():
             "ref_calc_propagator": ([_p, _f, _f, _f, _i, _fp], _i),
             "ref_calc_ring_detector": ([_p, _f, _f, _f, _f, _f, _f, C.c_char_p, _fp, _ip, _ip, _i], _i),
             "ref_cpu_scan": ([C.POINTER(_p), _i, _i, _fp, _i, _i, _fp], _i),
+            "ref_gpu_scan": ([_p, _i, _fp, _i, _i, _fp, C.POINTER(C.c_double)], _i),
             "ref_set_slice_thickness": ([_p, _i, _f], None),
             "ref_set_plasmon": ([_p, _i, _f, _f, _f, C.c_uint], None),
             "ref_sli_read_header": ([C.c_char_p, _ip, C.POINTER(C.c_ulonglong), _fp, C.c_char_p], _i),
@@ -283,6 +286,18 @@ def cpu_scan(objs, npos_xy: np.ndarray, nrepeat: int, ndetout: int) -> tuple[np.
     finally:
         torch.set_num_threads(nt0)
     return out, e
+
+
+def gpu_scan(obj, npos_xy: np.ndarray, nrepeat: int, ndetout: int) -> tuple[np.ndarray, float, int]:
+    """The reference GPU path (GPUMultislice, cuFFT) over positions x nrepeat
+    passes on one object set up for GPU code; returns (integrated detectors
+    [npos, ndetout], seconds, error code)."""
+    L = lib()
+    pos = np.ascontiguousarray(npos_xy, np.float32)
+    out = np.zeros((pos.shape[0], ndetout), np.float32)
+    sec = C.c_double(0.0)
+    e = L.ref_gpu_scan(obj.h, pos.shape[0], fptr(pos), nrepeat, ndetout, fptr(out), C.byref(sec))
+    return out, sec.value, e
 
 
 def pgr(nx, ny, a, b, c, ekv, Z, biso, occ, pos, thermal=0, absorb=0, abf=0.0, nrep=1, seed=0):

@@ -155,6 +155,33 @@ int ref_cpu_scan(void** objs, int nthreads, int npos, const float* pos, int nrep
 	return err.load();
 }
 
+// The reference GPU path (CJMultiSlice::GPUMultislice on cuFFT and the
+// ArrayOps kernels, src/JMultiSlice.cpp:4513-4677) driven per probe position
+// as the reference benchmark drives it (test/JMSBench1/multislice.cpp:551-620):
+// nrepeat frozen-phonon passes of OffsetIncomingWave + GPUMultislice (weight
+// 1/nrepeat, accumulating after the first), then GetResult of the integrated
+// detectors.  h: one object set up for GPU code.  *seconds: wall time of the
+// loop; every reference GPU call ends with a device synchronisation, so it is
+// the device time of the work.  out: npos * ndetout floats.
+int ref_gpu_scan(void* h, int npos, const float* pos, int nrepeat, int ndetout, float* out, double* seconds)
+{
+	RefJMS* jms = (RefJMS*)h;
+	const float w = 1.f / (float)nrepeat;
+	auto t0 = std::chrono::steady_clock::now();
+	for (int ip = 0; ip < npos; ip++) {
+		for (int ir = 0; ir < nrepeat; ir++) {
+			int e = jms->OffsetIncomingWave(_JMS_CODE_GPU, pos[2 * ip], pos[2 * ip + 1], 0.f, 0);
+			if (e == 0) e = jms->GPUMultislice(0, ir > 0 ? 1 : 0, w);
+			if (e != 0) return e;
+		}
+		int e = jms->GetResult(_JMS_CODE_GPU, _JMS_DETECT_INTEGRATED, out + (size_t)ip * ndetout, 0);
+		if (e != 0) return e;
+	}
+	auto t1 = std::chrono::steady_clock::now();
+	if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+	return 0;
+}
+
 void ref_set_slice_thickness(void* h, int islc, float t) { ((RefJMS*)h)->SetSliceThickness(islc, t); }
 void ref_set_plasmon(void* h, int use, float q_e, float q_c, float mfp, unsigned int nexmax)
 {
