@@ -209,10 +209,14 @@ int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* 
  * device array of 65536 floats (256 KiB per GPU, held until the process
  * ends); calls needing more than nwave * ndet * ceil(ny / 8) <= 65536 are
  * refused with 131.  All calls share that array, so calls that overlap on
- * the GPU race.  The first call on a device looks up the array's address
+ * the GPU race; JMS_ReadoutDetAvg with JMS_DETECT_INTEGRATED uses the same
+ * array on the library stream, so serialise it with calls of this function
+ * on other streams.  The first call on a device looks up the array's address
  * (cudaGetSymbolAddress) with that device current: make it before any stream
- * capture.  Returns 0, 1 (bad arguments), 2 (setup incomplete), 131, 132
- * (address lookup failed) or 133 (launch failed). */
+ * capture.  The address is kept per device and CUDA context; a call under a
+ * different context of the device looks it up again.  Returns 0, 1 (bad
+ * arguments), 2 (setup incomplete), 131, 132 (address lookup failed) or 133
+ * (launch failed). */
 int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream);
 /* Line-plan autotuner (no counterpart in the reference): times each candidate
  * FFT plan of nx (row passes) and ny (column passes) on nwave waves of the

@@ -19,28 +19,32 @@ using jms::JmsB200;
 // Library contexts: context 0 is the default instance of the reference's flat
 // interface; JMS_CreateContext adds more (each with its own grid, setup,
 // device buffers and stream), and JMS_SelectContext picks the one the flat
-// calls of the calling host thread act on.
+// calls of the calling host thread act on.  The table holds shared pointers
+// and every call works on its own copy, so a context that another thread
+// destroys meanwhile is freed only when the last call using it returns.
 namespace {
 std::mutex g_ctx_mu;
-std::vector<std::unique_ptr<JmsB200>> g_ctx;
+std::vector<std::shared_ptr<JmsB200>> g_ctx;
 thread_local int t_ctx = 0;
 
-JmsB200* ctx_get(int id)
+// with g_ctx_mu held
+std::shared_ptr<JmsB200> ctx_get(int id)
 {
-	if (g_ctx.empty()) g_ctx.emplace_back(new JmsB200());
-	return (id >= 0 && id < (int)g_ctx.size()) ? g_ctx[id].get() : nullptr;
+	if (g_ctx.empty()) g_ctx.emplace_back(std::make_shared<JmsB200>());
+	return (id >= 0 && id < (int)g_ctx.size()) ? g_ctx[id] : nullptr;
 }
 } // namespace
 
-static JmsB200& J()
+// the context of the calling thread (the default one if its context is gone)
+static std::shared_ptr<JmsB200> J()
 {
 	std::lock_guard<std::mutex> lock(g_ctx_mu);
-	JmsB200* j = ctx_get(t_ctx);
-	if (j == nullptr) {
+	std::shared_ptr<JmsB200> j = ctx_get(t_ctx);
+	if (!j) {
 		t_ctx = 0;
 		j = ctx_get(0);
 	}
-	return *j;
+	return j;
 }
 
 static jms::PgrGen& G()
@@ -56,25 +60,25 @@ extern "C" {
 
 float GetJMSVersion(void) { return 0.46f; }
 int SetJMSDebugLevel(int debuglevel) { int o = g_debug; g_debug = debuglevel; return o; }
-void SeedRngEx(int rngseed) { J().SeedRngEx(rngseed); }
+void SeedRngEx(int rngseed) { J()->SeedRngEx(rngseed); }
 
-float SetHighTension(float ht) { return J().SetHighTension(ht); }
-float GetHighTension(void) { return J().GetHighTension(); }
-float GetWaveLength(void) { return J().GetWaveLength(); }
-void SetSupercellSize(float* a0) { if (a0) J().SetSupercellSize(a0[0], a0[1], a0[2]); }
-void SetSupercellSizeABC(float a, float b, float c) { J().SetSupercellSize(a, b, c); }
-void SetSliceThickness(int islc, float fthickness) { J().SetSliceThickness(islc, fthickness); }
-void DiffractionDescan(int bActivate) { J().DiffractionDescan(bActivate != 0); }
+float SetHighTension(float ht) { return J()->SetHighTension(ht); }
+float GetHighTension(void) { return J()->GetHighTension(); }
+float GetWaveLength(void) { return J()->GetWaveLength(); }
+void SetSupercellSize(float* a0) { if (a0) J()->SetSupercellSize(a0[0], a0[1], a0[2]); }
+void SetSupercellSizeABC(float a, float b, float c) { J()->SetSupercellSize(a, b, c); }
+void SetSliceThickness(int islc, float fthickness) { J()->SetSliceThickness(islc, fthickness); }
+void DiffractionDescan(int bActivate) { J()->DiffractionDescan(bActivate != 0); }
 void SetPlasmonMC(int bActivate, float fq_e, float fq_c, float fmfp, unsigned int nexmax)
-{ J().SetPlasmonMC(bActivate != 0, fq_e, fq_c, fmfp, nexmax); }
-void SetDiffractionDescanN(int whichcode, int ndescanx, int ndescany, int) { J().SetDiffractionDescanN(whichcode, ndescanx, ndescany); }
-void SetDiffractionDescan(int whichcode, float descanx, float descany, int) { J().SetDiffractionDescan(whichcode, descanx, descany); }
-void SetDiffractionDescanMRad(int whichcode, float descanx, float descany, int) { J().SetDiffractionDescanMRad(whichcode, descanx, descany); }
+{ J()->SetPlasmonMC(bActivate != 0, fq_e, fq_c, fmfp, nexmax); }
+void SetDiffractionDescanN(int whichcode, int ndescanx, int ndescany, int) { J()->SetDiffractionDescanN(whichcode, ndescanx, ndescany); }
+void SetDiffractionDescan(int whichcode, float descanx, float descany, int) { J()->SetDiffractionDescan(whichcode, descanx, descany); }
+void SetDiffractionDescanMRad(int whichcode, float descanx, float descany, int) { J()->SetDiffractionDescanMRad(whichcode, descanx, descany); }
 
-void SetGridSize(int nx, int ny) { J().SetGridSize(nx, ny); }
-void GetGridSize(int* nx, int* ny) { int a = 0, b = 0; J().GetGridSize(a, b); if (nx) *nx = a; if (ny) *ny = b; }
-int GetDetetionSliceNum(void) { return J().GetDetetionSliceNum(); }
-int GetDetNum(void) { return J().GetDetNum(); }
+void SetGridSize(int nx, int ny) { J()->SetGridSize(nx, ny); }
+void GetGridSize(int* nx, int* ny) { int a = 0, b = 0; J()->GetGridSize(a, b); if (nx) *nx = a; if (ny) *ny = b; }
+int GetDetetionSliceNum(void) { return J()->GetDetetionSliceNum(); }
+int GetDetNum(void) { return J()->GetDetNum(); }
 int GetCPUNum(void) { return (int)std::thread::hardware_concurrency(); }
 int GetGPUNum(void) { int n = 0; if (cudaGetDeviceCount(&n) != cudaSuccess) return 0; return n; }
 int GetGPUName(int idev, char* name)
@@ -85,8 +89,8 @@ int GetGPUName(int idev, char* name)
 	name[255] = 0;
 	return 0;
 }
-int GetCurrentGPU(void) { return J().GetCurrentGPU(); }
-int SetCurrentGPU(int idev) { return J().SetCurrentGPU(idev); }
+int GetCurrentGPU(void) { return J()->GetCurrentGPU(); }
+int SetCurrentGPU(int idev) { return J()->SetCurrentGPU(idev); }
 int GetGPUStats(int idev, int* iCMajor, int* iCMinor, int* iMaxThread, int64_t* memtotal, int64_t* memfree)
 {
 	cudaDeviceProp p;
@@ -104,29 +108,29 @@ int GetGPUStats(int idev, int* iCMajor, int* iCMinor, int* iMaxThread, int64_t* 
 	if (memfree) *memfree = (int64_t)f;
 	return 0;
 }
-int GetUnscrambleHash(unsigned int* phash) { return J().GetUnscrambleHash(phash); }
-float GetImageAveragingWeight(int whichcode, int iThread) { return J().GetImageAveragingWeight(whichcode, iThread); }
-float GetWaveAveragingWeight(int whichcode, int iThread) { return J().GetWaveAveragingWeight(whichcode, iThread); }
+int GetUnscrambleHash(unsigned int* phash) { return J()->GetUnscrambleHash(phash); }
+float GetImageAveragingWeight(int whichcode, int iThread) { return J()->GetImageAveragingWeight(whichcode, iThread); }
+float GetWaveAveragingWeight(int whichcode, int iThread) { return J()->GetWaveAveragingWeight(whichcode, iThread); }
 
 int PhaseGratingSetup(int whichcode, int nx, int ny, int nslc, int nvarmax, int* nslcvar)
-{ return J().PhaseGratingSetup(whichcode, nx, ny, nslc, nvarmax, nslcvar); }
-int ObjectSliceSetup(int nobjslc, int* objslc) { return J().ObjectSliceSetup(nobjslc, objslc); }
-int PropagatorSetup(int whichcode, int npro, int* proidx) { return J().PropagatorSetup(whichcode, npro, proidx); }
+{ return J()->PhaseGratingSetup(whichcode, nx, ny, nslc, nvarmax, nslcvar); }
+int ObjectSliceSetup(int nobjslc, int* objslc) { return J()->ObjectSliceSetup(nobjslc, objslc); }
+int PropagatorSetup(int whichcode, int npro, int* proidx) { return J()->PropagatorSetup(whichcode, npro, proidx); }
 int DetectorSetup(int whichcode, int ndetper, int ndetint, int imagedet, int nthreads_CPU)
-{ return J().DetectorSetup(whichcode, ndetper, ndetint, imagedet, nthreads_CPU); }
-int InitCore(int whichcode, int nCPUthreads) { return J().InitCore(whichcode, nCPUthreads); }
-int SetIncidentWave(int whichcode, float* wav) { return J().SetIncidentWave(whichcode, wav, false); }
+{ return J()->DetectorSetup(whichcode, ndetper, ndetint, imagedet, nthreads_CPU); }
+int InitCore(int whichcode, int nCPUthreads) { return J()->InitCore(whichcode, nCPUthreads); }
+int SetIncidentWave(int whichcode, float* wav) { return J()->SetIncidentWave(whichcode, wav, false); }
 int SetIncidentWavePhaseplate(int whichcode, float* ppl, int bTranspose)
-{ return J().SetIncidentWavePhaseplate(whichcode, ppl, bTranspose != 0); }
-int ZeroIncidentWavePhaseplate(int whichcode) { return J().ZeroIncidentWavePhaseplate(whichcode); }
+{ return J()->SetIncidentWavePhaseplate(whichcode, ppl, bTranspose != 0); }
+int ZeroIncidentWavePhaseplate(int whichcode) { return J()->ZeroIncidentWavePhaseplate(whichcode); }
 int SetSlicePhaseGratings(int whichcode, int islc, int nvar, float* pgr)
-{ return J().SetPhaseGratingData(whichcode, islc, nvar, pgr); }
-int SetPropagatorData(int whichcode, int ipro, float* pro) { return J().SetPropagatorData(whichcode, ipro, pro); }
+{ return J()->SetPhaseGratingData(whichcode, islc, nvar, pgr); }
+int SetPropagatorData(int whichcode, int ipro, float* pro) { return J()->SetPropagatorData(whichcode, ipro, pro); }
 int SetDetectorData(int whichcode, int idet, float* det, int msklen, int* msk)
-{ return J().SetDetectorData(whichcode, idet, det, msklen, msk); }
-int SetGPUPgrLoading(int npgrload) { return J().SetGPUPgrLoading(npgrload); }
-int ResetImageAveraging(int whichcode, int iThread) { return J().ResetImageAveraging(whichcode, iThread); }
-int ResetWaveAveraging(int whichcode, int iThread) { return J().ResetWaveAveraging(whichcode, iThread); }
+{ return J()->SetDetectorData(whichcode, idet, det, msklen, msk); }
+int SetGPUPgrLoading(int npgrload) { return J()->SetGPUPgrLoading(npgrload); }
+int ResetImageAveraging(int whichcode, int iThread) { return J()->ResetImageAveraging(whichcode, iThread); }
+int ResetWaveAveraging(int whichcode, int iThread) { return J()->ResetWaveAveraging(whichcode, iThread); }
 
 int CalculateProbeWaveFourier(JMSProbeParams* prm, float* wav)
 {
@@ -142,41 +146,41 @@ int CalculateProbeWaveFourier(JMSProbeParams* prm, float* wav)
 	p.btx = prm->m_btx;
 	p.bty = prm->m_bty;
 	if (prm->m_abrr_coeff) std::memcpy(p.abrr, prm->m_abrr_coeff, sizeof(p.abrr));
-	return J().CalculateProbeWaveFourier(p, wav);
+	return J()->CalculateProbeWaveFourier(p, wav);
 }
-int SetIncomingWaveGPU(float* wav, int bTranspose) { return J().SetIncomingWaveGPU(wav, bTranspose != 0); }
+int SetIncomingWaveGPU(float* wav, int bTranspose) { return J()->SetIncomingWaveGPU(wav, bTranspose != 0); }
 int SetIncomingWaveCPU(float*, int, int) { return 1; }
 int CalculatePropagator(float fthick, float otx, float oty, float* pro, int ntype)
-{ return J().CalculatePropagator(fthick, otx, oty, pro, ntype); }
+{ return J()->CalculatePropagator(fthick, otx, oty, pro, ntype); }
 int CalculateRingDetector(float beta0, float beta1, float phi0, float phi1, float theta0x, float theta0y,
 	const char* sdsprofile, float* det, int* msklen, int* msk, int kmom1)
 {
 	// the reference's flat interface passes theta0x twice (src/JMultiSliceLib.cpp:254);
 	// here theta0y reaches the class as intended
-	return J().CalculateRingDetector(beta0, beta1, phi0, phi1, theta0x, theta0y, sdsprofile, det, msklen, msk, kmom1);
+	return J()->CalculateRingDetector(beta0, beta1, phi0, phi1, theta0x, theta0y, sdsprofile, det, msklen, msk, kmom1);
 }
 int OffsetIncomingWave(int whichcode, float dx, float dy, float dz, int iThread, int ibtx, int ibty)
-{ return J().OffsetIncomingWave(whichcode, dx, dy, dz, iThread, ibtx, ibty, true); }
+{ return J()->OffsetIncomingWave(whichcode, dx, dy, dz, iThread, ibtx, ibty, true); }
 int CPUMultislice(int, int, float, int) { return 1; }
-int GPUMultislice(int islc0, int accmode, float weight) { return J().GPUMultislice(islc0, accmode, weight); }
+int GPUMultislice(int islc0, int accmode, float weight) { return J()->GPUMultislice(islc0, accmode, weight); }
 int GetResult(int whichcode, int whichresult, float* dst, int iThread)
-{ return J().GetResult(whichcode, whichresult, dst, iThread); }
+{ return J()->GetResult(whichcode, whichresult, dst, iThread); }
 int GetAvgResult(int whichcode, int whichresult, float* dst, float* wgt, int iThread)
-{ return J().GetAvgResult(whichcode, whichresult, dst, wgt, iThread); }
+{ return J()->GetAvgResult(whichcode, whichresult, dst, wgt, iThread); }
 int ClearDetMem_h(int) { return 1; }
-int ClearDetMem_d(void) { return J().ClearDetMem_d(); }
-int Cleanup(void) { return J().Cleanup(); }
+int ClearDetMem_d(void) { return J()->ClearDetMem_d(); }
+int Cleanup(void) { return J()->Cleanup(); }
 void FreeLibMem(void) {}
 
-int JMS_SetStream(void* stream) { return J().SetStream((cudaStream_t)stream); }
+int JMS_SetStream(void* stream) { return J()->SetStream((cudaStream_t)stream); }
 int JMS_ScanGPU(int npos, const float* pos, float dz, int npass, const int* varseq, float* out_int, float* out_bin,
 	int bin)
-{ return J().ScanGPU(npos, pos, dz, npass, varseq, out_int, out_bin, bin); }
+{ return J()->ScanGPU(npos, pos, dz, npass, varseq, out_int, out_bin, bin); }
 int JMS_ScanGPUDevice(int npos, const float* d_pos, float dz, int npass, const int* varseq, double* d_out_int,
 	float* d_out_bin, int bin)
-{ return J().ScanGPUDevice(npos, d_pos, dz, npass, varseq, d_out_int, d_out_bin, bin); }
-int JMS_SetScanBatch(int nwave) { return J().SetScanBatch(nwave); }
-int JMS_SetPassFusion(int on) { return J().SetPassFusion(on); }
+{ return J()->ScanGPUDevice(npos, d_pos, dz, npass, varseq, d_out_int, d_out_bin, bin); }
+int JMS_SetScanBatch(int nwave) { return J()->SetScanBatch(nwave); }
+int JMS_SetPassFusion(int on) { return J()->SetPassFusion(on); }
 
 // Multi-fidelity frozen-phonon scan: the control-variate estimate
 //   est = f(c0) + (npass - 1) / npass * (mean_{c1..} g - g(c0))
@@ -188,7 +192,7 @@ int JMS_SetPassFusion(int on) { return J().SetPassFusion(on); }
 int JMS_ScanMultiFidelityDevice(int ctx_full, int ctx_low, int npos, const float* d_pos, float dz, int npass,
 	const int* varseq, double* d_out_int)
 {
-	JmsB200 *F = nullptr, *Lo = nullptr;
+	std::shared_ptr<JmsB200> F, Lo;
 	{
 		std::lock_guard<std::mutex> lock(g_ctx_mu);
 		F = ctx_get(ctx_full);
@@ -231,7 +235,7 @@ int JMS_ScanMultiFidelity(int ctx_full, int ctx_low, int npos, const float* pos,
 	const int* varseq, float* out_int)
 {
 	if (npos < 1 || pos == nullptr || out_int == nullptr) return 1;
-	JmsB200* F = nullptr;
+	std::shared_ptr<JmsB200> F;
 	{
 		std::lock_guard<std::mutex> lock(g_ctx_mu);
 		F = ctx_get(ctx_full);
@@ -255,46 +259,46 @@ int JMS_ScanMultiFidelity(int ctx_full, int ctx_low, int npos, const float* pos,
 	for (size_t i = 0; i < n; i++) out_int[i] = (float)h[i];
 	return 0;
 }
-long long JMS_KernelLaunches(void) { return J().KernelLaunches(); }
-void JMS_SetPassTiming(int on) { J().SetPassTiming(on); }
+long long JMS_KernelLaunches(void) { return J()->KernelLaunches(); }
+void JMS_SetPassTiming(int on) { J()->SetPassTiming(on); }
 int JMS_PassTiming(double* ms_col, long long* n_col, double* ms_row, long long* n_row)
-{ return J().PassTiming(ms_col, n_col, ms_row, n_row); }
+{ return J()->PassTiming(ms_col, n_col, ms_row, n_row); }
 int JMS_ReadoutDetectorsNoAlloc(const float* d_wav, int nwave, double* d_out, void* stream)
-{ return J().ReadoutDetectorsNoAlloc(d_wav, nwave, d_out, (cudaStream_t)stream); }
+{ return J()->ReadoutDetectorsNoAlloc(d_wav, nwave, d_out, (cudaStream_t)stream); }
 int JMS_Autotune(int nwave, int reps, float* ms_row, float* ms_col, int* irow, int* icol)
-{ return J().Autotune(nwave, reps, ms_row, ms_col, irow, icol); }
-int JMS_SelectPlans(int irow, int icol) { return J().SelectPlans(irow, icol); }
+{ return J()->Autotune(nwave, reps, ms_row, ms_col, irow, icol); }
+int JMS_SelectPlans(int irow, int icol) { return J()->SelectPlans(irow, icol); }
 int JMS_PlanCount(int n) { return jms::plan_count(n); }
 int JMS_PlanName(int axis, char* name, int len)
 {
 	if (!name || len < 1) return 1;
-	std::strncpy(name, J().PlanName(axis), (size_t)len - 1);
+	std::strncpy(name, J()->PlanName(axis), (size_t)len - 1);
 	name[len - 1] = 0;
 	return 0;
 }
 int JMS_GridSupported(int nx, int ny) { return (jms::pass_supported(nx) && jms::pass_supported(ny)) ? 1 : 0; }
-int JMS_SetPrecision(int mode) { return J().SetPrecision(mode); }
-int JMS_GetPrecision(void) { return J().GetPrecision(); }
-int JMS_TcStatus(void) { return J().TcStatus(); }
-long long JMS_TcLaunches(void) { return J().TcLaunches(); }
+int JMS_SetPrecision(int mode) { return J()->SetPrecision(mode); }
+int JMS_GetPrecision(void) { return J()->GetPrecision(); }
+int JMS_TcStatus(void) { return J()->TcStatus(); }
+long long JMS_TcLaunches(void) { return J()->TcLaunches(); }
 
 int JMS_ReadoutDetAvg(int whichcode, int whichresult, float* dst, float* weight)
-{ return J().ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }
+{ return J()->ReadoutDetAvg(whichcode, whichresult, dst, weight, 0); }
 
 int JMS_CreateContext(void)
 {
 	std::lock_guard<std::mutex> lock(g_ctx_mu);
 	ctx_get(0);
 	for (size_t i = 1; i < g_ctx.size(); i++)
-		if (!g_ctx[i]) { g_ctx[i].reset(new JmsB200()); return (int)i; }
-	g_ctx.emplace_back(new JmsB200());
+		if (!g_ctx[i]) { g_ctx[i] = std::make_shared<JmsB200>(); return (int)i; }
+	g_ctx.emplace_back(std::make_shared<JmsB200>());
 	return (int)g_ctx.size() - 1;
 }
 
 int JMS_SelectContext(int id)
 {
 	std::lock_guard<std::mutex> lock(g_ctx_mu);
-	if (ctx_get(id) == nullptr) return -1;
+	if (!ctx_get(id)) return -1;
 	const int old = t_ctx;
 	t_ctx = id;
 	return old;
@@ -302,14 +306,14 @@ int JMS_SelectContext(int id)
 
 int JMS_DestroyContext(int id)
 {
-	std::unique_ptr<JmsB200> victim;
+	std::shared_ptr<JmsB200> victim;
 	{
 		std::lock_guard<std::mutex> lock(g_ctx_mu);
-		if (id <= 0 || ctx_get(id) == nullptr) return 1;
+		if (id <= 0 || !ctx_get(id)) return 1;
 		victim = std::move(g_ctx[id]);
 		if (t_ctx == id) t_ctx = 0;
 	}
-	return 0;   // the context is freed here, outside the lock
+	return 0;   // freed here, outside the lock, unless a call on another thread still holds it
 }
 
 // ---- CUDA graphs over contexts -------------------------------------------
@@ -333,8 +337,8 @@ int JMS_GraphBegin(int nctx, const int* ctx)
 	{
 		std::lock_guard<std::mutex> lk(g_ctx_mu);
 		for (int i = 0; i < nctx; i++) {
-			JmsB200* j = ctx_get(ctx[i]);
-			if (j == nullptr) return 1;
+			std::shared_ptr<JmsB200> j = ctx_get(ctx[i]);
+			if (!j) return 1;
 			if (j->Stream() == nullptr) return 2;   // the context needs its stream (InitCore)
 			for (cudaStream_t q : streams)
 				if (q == j->Stream()) return 1;
@@ -413,11 +417,11 @@ int JMS_SliLoadSlice(const char* path, int islc)
 	int e = JMS_SliReadHeader(path, &h);
 	if (e) return e;
 	int npgx = 0, npgy = 0;
-	if (J().GratingSlot(islc, 0, 1, &npgx, &npgy) == nullptr) return 1;
+	if (J()->GratingSlot(islc, 0, 1, &npgx, &npgy) == nullptr) return 1;
 	if (h.nx != npgx || h.ny != npgy) return 7;
 	std::vector<float> buf((size_t)2 * h.nx * h.ny * h.nvar);
 	if ((e = JMS_SliReadData(path, buf.data()))) return e;
-	return J().SetPhaseGratingData(jms::CODE_GPU, islc, h.nvar, buf.data());
+	return J()->SetPhaseGratingData(jms::CODE_GPU, islc, h.nvar, buf.data());
 }
 
 int JMS_PgrSetup(int nx, int ny, float a, float b, float ekv, int thermal, int bwl_pot, int bwl_pgr)
@@ -440,10 +444,10 @@ int JMS_PgrCalculate(int natom, const float* atoms, float cz, int ngr, unsigned 
 	float2* dst = nullptr;
 	if (islc >= 0) {
 		int npgx = 0, npgy = 0;
-		dst = J().GratingSlot(islc, ivar0, ngr, &npgx, &npgy);
+		dst = J()->GratingSlot(islc, ivar0, ngr, &npgx, &npgy);
 		if (dst == nullptr || npgx != G().nx() || npgy != G().ny()) return 9;
 	}
-	cudaStream_t s = g_pgr_stream ? g_pgr_stream : J().Stream();
+	cudaStream_t s = g_pgr_stream ? g_pgr_stream : J()->Stream();
 	G().SetStream(s);
 	int e = G().Calculate(natom, atoms, cz, ngr, seed, dst, pgr);
 	// before InitCore the context has no stream of its own yet, and the one it

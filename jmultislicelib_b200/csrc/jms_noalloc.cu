@@ -18,11 +18,18 @@
 //     example from two streams) race on it;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress while that device is current; make that first call
-//     before any stream capture.  Later calls on the device reuse the address.
+//     before any stream capture.  Later calls on the device reuse the address
+//     as long as the same CUDA context is current there; a call under another
+//     context of that device (after cudaDeviceReset, or a caller-made
+//     context) looks the address up again;
+//   - JMS_ReadoutDetAvg with JMS_DETECT_INTEGRATED uses the same array on the
+//     library's stream, so callers serialise it with calls of this entry point
+//     on other streams.
 // Every partial sum the reduction reads is written earlier in the same call,
 // so nothing has to be cleared between calls.
 #include "jms_kernels.h"
 
+#include <cuda.h>
 #include <cstdio>
 #include <mutex>
 
@@ -86,16 +93,39 @@ __global__ void k_reduce_noalloc(const float* __restrict__ partial, int n, int n
 	out[i] = s;
 }
 
+// The driver context current on the calling thread (nullptr if none or if the
+// driver entry point is unavailable), through the runtime's driver entry-point
+// query, so the library needs no link to the driver library.
+static CUcontext current_context()
+{
+	typedef CUresult (*GetCurrent)(CUcontext*);
+	static GetCurrent fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, []() {
+		void* f = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+			q == cudaDriverEntryPointSuccess)
+			fn = (GetCurrent)f;
+	});
+	CUcontext c = nullptr;
+	if (fn == nullptr || fn(&c) != CUDA_SUCCESS) return nullptr;
+	return c;
+}
+
 // Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress; host code cannot use the symbol itself).
+// per device and context (cudaGetSymbolAddress; host code cannot use the
+// symbol itself, and the address belongs to the context it was made in).
 static int noalloc_scratch(float** ptr)
 {
 	static std::mutex mu;
 	static float* addr[kNoAllocMaxDevices] = {nullptr};
+	static CUcontext owner[kNoAllocMaxDevices] = {nullptr};
 	int dev = -1;
 	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return 1;
+	const CUcontext ctx = current_context();
 	std::lock_guard<std::mutex> lock(mu);
-	if (addr[dev] == nullptr) {
+	if (addr[dev] == nullptr || owner[dev] != ctx) {
 		void* p = nullptr;
 		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
 		if (e != cudaSuccess || p == nullptr) {
@@ -104,6 +134,7 @@ static int noalloc_scratch(float** ptr)
 			return 2;
 		}
 		addr[dev] = (float*)p;
+		owner[dev] = current_context();   // the context the lookup ran in (made current by it if none was)
 	}
 	*ptr = addr[dev];
 	return 0;

@@ -71,6 +71,37 @@ def test_no_alloc_readout_matches_regular_path_twice():
         assert rel.max() < TOL, (call, got, expect)
 
 
+def test_no_alloc_readout_on_a_caller_stream():
+    """The wave is written on a stream of the caller's and the readout is
+    enqueued on that stream: the result must follow the write, twice."""
+    import torch
+
+    import jmultislicelib_b200 as jb
+
+    J = jb.JMS()
+    nx, ny, nobj = 128, 96, 4
+    ndet = _setup(J, nx, ny, nobj)
+    rng = np.random.default_rng(6)
+    s = torch.cuda.Stream()
+    out = torch.zeros(ndet, dtype=torch.float64, device="cuda")
+    d_wav = torch.zeros(2 * nx * ny, dtype=torch.float32, device="cuda")
+    for call in range(2):
+        wav = (rng.normal(size=(ny, nx)) + 1j * rng.normal(size=(ny, nx))).astype(np.complex64)
+        wav /= np.sqrt((np.abs(wav) ** 2).sum())
+        expect = _regular_readout(J, wav, nobj, ndet)
+        h_wav = torch.from_numpy(wav.view(np.float32).ravel().copy()).pin_memory()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(s):
+            d_wav.copy_(h_wav, non_blocking=True)     # the wave arrives on the caller's stream
+            e = J.L.JMS_ReadoutDetectorsNoAlloc(d_wav.data_ptr(), 1, out.data_ptr(), C.c_void_p(s.cuda_stream))
+            got_d = out.clone()
+        s.synchronize()
+        assert e == 0, e
+        got = got_d.cpu().numpy()
+        rel = np.abs(got - expect) / np.maximum(np.abs(expect), 1e-30)
+        assert rel.max() < TOL, (call, got, expect)
+
+
 def test_no_alloc_readout_refuses_oversize_request():
     import torch
 
