@@ -456,6 +456,18 @@ def run_ours(args):
                 "traffic": traffic_from_profiles(kind, waves), "bytes_per_launch": algo,
                 "avg_launch_us": avg_s * 1e6, "col_pass_us": 1e3 * mc.value / max(nc.value, 1),
                 "row_pass_us": 1e3 * mr.value / max(nr.value, 1)}
+        # the bytes the band-pruned design must move per slice of the whole step:
+        # each wave's live rows (rows where the propagator is nonzero) read and
+        # written once by each of the two passes, each configuration's grating
+        # and the propagator read once per launch
+        live = float(np.count_nonzero(np.abs(pro).max(axis=1) > 0)) / cfg["ny"]
+        pruned = waves * 32 * N * live + kp * 8 * N + 8 * N
+        slice_s = (ms / args.steps) / 1e3 / cfg["nobj"] * (waves / (npos_step * npass))
+        roof["pruned"] = {"bytes_per_slice": pruned, "live_row_fraction": live,
+                          "achieved": pruned / slice_s / 1e9, "frac": pruned / slice_s / 1e9 / hbm,
+                          "note": f"one slice of {waves} waves in the timed step (all launches of the slice, "
+                                  "readout planes included) against the bytes a band-pruned two-pass step must "
+                                  "move; the pass rows above count 24 N per wave and pass"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",

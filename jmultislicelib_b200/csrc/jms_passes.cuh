@@ -629,8 +629,25 @@ k_row_pass_read(const PassArgs p)
 	row_pass_body<PL, true>(p);
 }
 
-// Column pass: IFT_y -> real-space readout (plane) -> x t -> FT_y.
-template <class PL, bool READ>
+// Live rows of a column-pass thread as a bit mask: bit m is set when row
+// y = j + B m (m < A) lies outside the band gap (k1, k2), i.e. y <= k1 or
+// y >= k2.  One mask per thread replaces a comparison per element.
+template <int A, int B>
+__device__ __forceinline__ unsigned live_rows(int j, int k1, int k2)
+{
+	static_assert(A <= 32, "one bit per value");
+	const int lo = k1 >= j ? min((k1 - j) / B, A - 1) : -1;          // last m with y <= k1
+	const int hi = k2 > j ? min((k2 - j + B - 1) / B, 32) : 0;       // first m with y >= k2
+	const unsigned low = lo < 0 ? 0u : (lo >= 31 ? 0xffffffffu : ((2u << lo) - 1u));
+	const unsigned high = hi >= 32 ? 0u : (0xffffffffu << hi);
+	return low | high;
+}
+
+// Column pass: IFT_y -> real-space readout (plane) -> x t -> FT_y.  NXC is the
+// row stride when it is known at compile time (square grids, nx = N), so the
+// element offsets of the wave and grating accesses are constants; 0 reads it
+// from the arguments.
+template <class PL, bool READ, int NXC>
 __global__ void __launch_bounds__(PL::CC * PL::TMAX)
 k_col_pass(const PassArgs p)
 {
@@ -638,8 +655,8 @@ k_col_pass(const PassArgs p)
 	using T = ColTile<C>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
-	const int nval = min(C, p.nx - col0);
-	const int nx = p.nx;
+	const int nx = NXC > 0 ? NXC : p.nx;
+	const int nval = min(C, nx - col0);
 	float2* W = p.work + (long long)b * p.wstride + col0;
 	float2 v[PL::RM];
 	#pragma unroll
@@ -651,11 +668,10 @@ k_col_pass(const PassArgs p)
 	const int stride = PL::B * nx;
 	if (c < nval && j < PL::T) {
 		const float2* src = W + j * nx + c;
+		const unsigned lin = live_rows<PL::A, PL::B>(j, p.in_k1, p.in_k2);
 		#pragma unroll
-		for (int m = 0; m < PL::A; m++) {
-			const int y = j + PL::B * m;
-			if (y <= p.in_k1 || y >= p.in_k2) v[m] = src[m * stride];
-		}
+		for (int m = 0; m < PL::A; m++)
+			if (lin & (1u << m)) v[m] = src[m * stride];
 	}
 	PL::template to_mid<true, T>(v, sm, p.twy, tid);
 	{
@@ -701,11 +717,10 @@ k_col_pass(const PassArgs p)
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
 		float2* dst = W + j * nx + c;
+		const unsigned lout = live_rows<PL::A, PL::B>(j, p.out_k1, p.out_k2);
 		#pragma unroll
-		for (int m = 0; m < PL::A; m++) {
-			const int y = j + PL::B * m;
-			if (y <= p.out_k1 || y >= p.out_k2) dst[m * stride] = v[m];
-		}
+		for (int m = 0; m < PL::A; m++)
+			if (lout & (1u << m)) dst[m * stride] = v[m];
 	}
 }
 
@@ -1010,7 +1025,10 @@ cudaError_t launch_col_t(const PassArgs& p, cudaStream_t s)
 	constexpr int C = PL::CC;
 	constexpr int smem = PL::template smem_elems<ColTile<C>>() * (int)sizeof(float2);
 	const dim3 grid((p.nx + C - 1) / C, p.nwave);
-	if (p.plane >= 0) return launch_k(k_col_pass<PL, true>, grid, C * PL::TMAX, smem, p, s);
+	if (p.plane >= 0) {
+		if (p.nx == PL::N) return launch_k(k_col_pass<PL, true, PL::N>, grid, C * PL::TMAX, smem, p, s);
+		return launch_k(k_col_pass<PL, true, 0>, grid, C * PL::TMAX, smem, p, s);
+	}
 	if constexpr (PL::PIPE) {
 		if (p.nx % 2 == 0) {
 			const int ncb = (p.nx + C - 1) / C;
@@ -1019,7 +1037,8 @@ cudaError_t launch_col_t(const PassArgs& p, cudaStream_t s)
 			return launch_pipe(k_col_pass_pipe<PL>, C * PL::TMAX, smem_p, ntiles, s, p, ncb, (int)ntiles);
 		}
 	}
-	return launch_k(k_col_pass<PL, false>, grid, C * PL::TMAX, smem, p, s);
+	if (p.nx == PL::N) return launch_k(k_col_pass<PL, false, PL::N>, grid, C * PL::TMAX, smem, p, s);
+	return launch_k(k_col_pass<PL, false, 0>, grid, C * PL::TMAX, smem, p, s);
 }
 template <class PL>
 cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
