@@ -766,24 +766,28 @@ def run_cv(args):
     tr_cfg = configs(args.cv_train_configs)
     tr_pos = (cell0 + rng.uniform(0, S.A_CELL, (args.cv_train_positions, 2))).astype(np.float32)
     d_tr = torch.from_numpy(tr_pos).cuda()
+    # surrogate input: one channel per readout interval of the depth, a 64 x 64-
+    # pixel window around the probe averaged to 16 x 16
+    nbins, pool = args.cv_bins, args.cv_pool
+    size = SG.PATCH // pool
     X, Y = [], []
     t_gen = 0.0
     for v in tr_cfg:
-        maps = SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v)
-        X.append(SG.patches(maps, tr_pos, sp.a, sp.b).astype(np.float32))
+        maps = SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v, nbins)
+        X.append(SG.patches(maps, tr_pos, sp.a, sp.b, pool=pool).astype(np.float32))
         y, dt = SG.timed(lambda: SG.signals(J, d_tr, len(tr_pos), v, planes))
         Y.append(y)
         t_gen += dt
     # the surrogate learns the phonon fluctuation at a fixed position: inputs
     # and targets are deviations from their mean over the configurations
-    X = np.stack(X)                    # [config, position, 3, 64, 64]
+    X = np.stack(X)                    # [config, position, nbins, size, size]
     Y = np.stack(Y)                    # [config, position, nout]
     X -= X.mean(axis=0, keepdims=True)
     Y -= Y.mean(axis=0, keepdims=True)
     nval = max(2, len(tr_cfg) // 8)    # held-out configurations: early stopping and beta
     Xt, Yt = X[nval:].reshape(-1, *X.shape[2:]), Y[nval:].reshape(-1, nout)
     Xv, Yv = X[:nval].reshape(-1, *X.shape[2:]), Y[:nval].reshape(-1, nout)
-    cv = SG.ControlVariate(nout, batch=256, seed=1)
+    cv = SG.ControlVariate(nout, batch=256, seed=1, cin=nbins, size=size, relu=not args.cv_linear)
     hist, t_train = SG.timed(lambda: cv.fit(Xt, Yt, Xv, Yv, epochs=args.cv_epochs))
     # evaluation: 8x8 subset of the raster, 64 fresh configurations
     ev_pos = np.ascontiguousarray(raster.reshape(64, 64, 2)[::8, ::8].reshape(-1, 2))
@@ -791,13 +795,14 @@ def run_cv(args):
     ev_cfg = configs(64)
     F = np.zeros((64, len(ev_pos), nout))
     G = np.zeros_like(F)
-    P = np.zeros((64, len(ev_pos), 3, SG.PATCH, SG.PATCH), np.float32)
+    P = np.zeros((64, len(ev_pos), nbins, size, size), np.float32)
     t_full = t_sur = t_patch = 0.0
     for k, v in enumerate(ev_cfg):
         F[k], dt = SG.timed(lambda: SG.signals(J, d_ev, len(ev_pos), v, planes))
         t_full += dt
         t0 = time.perf_counter()
-        P[k] = SG.patches(SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v), ev_pos, sp.a, sp.b)
+        P[k] = SG.patches(SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v, nbins), ev_pos, sp.a, sp.b,
+                          pool=pool)
         t_patch += time.perf_counter() - t0
     P -= P.mean(axis=0, keepdims=True)
     G, t_sur = SG.timed(lambda: cv.predict(P.reshape(-1, *P.shape[2:])).reshape(F.shape))
@@ -815,6 +820,9 @@ def run_cv(args):
             "data": "synthetic",
             "config": {"workload": "512^2 scan specimen, 8x8 positions, 64 phonon configurations as ground truth, "
                                    "estimator 4 full + surrogate on 64",
+                       "input": f"{nbins} depth bins x {size} x {size} (64 x 64-pixel window averaged "
+                                f"{pool} x {pool})", "relu": not args.cv_linear,
+                       "train_configs": int(args.cv_train_configs),
                        "train_pairs": int(Xt.shape[0]), "validation_pairs": int(Xv.shape[0]),
                        "epochs": args.cv_epochs, "outputs": nout},
             "err_plain4_per_det": [float(v) for v in e_plain.mean(axis=0)],
@@ -1386,6 +1394,9 @@ def main():
     ap.add_argument("--cv-train-configs", type=int, default=32)
     ap.add_argument("--cv-train-positions", type=int, default=625)
     ap.add_argument("--cv-epochs", type=int, default=30)
+    ap.add_argument("--cv-bins", type=int, default=10, help="depth bins (input channels) of the surrogate")
+    ap.add_argument("--cv-pool", type=int, default=4, help="pixel blocks averaged in the surrogate's input")
+    ap.add_argument("--cv-linear", action="store_true", help="surrogate convolutions without ReLU")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

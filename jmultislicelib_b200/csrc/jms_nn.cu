@@ -2,12 +2,12 @@
 // storage, FP32 accumulation), training and inference.
 //
 // The surrogate maps a local projected-potential patch around the probe
-// (3 channels x 64 x 64) to the integrated detector signals at the readout
-// thicknesses.  Layers: three 3x3 convolutions of stride 2 and padding 1 with
-// ReLU (BF16 activations and weights), a global average pool, and a linear
-// layer (FP32).  The host side (jmultislicelib_b200/surrogate.py) owns the
-// buffers and the training loop; these kernels are the building blocks:
-// forward, both backward products, loss, Adam.
+// (one channel per depth bin) to the integrated detector signals at the
+// readout thicknesses.  Layers: 3x3 convolutions of stride 2 and padding 1,
+// with or without ReLU (BF16 activations and weights), a global average pool,
+// and a linear layer (FP32).  The host side (jmultislicelib_b200/surrogate.py)
+// owns the buffers and the training loop; these kernels are the building
+// blocks: forward, both backward products, loss, Adam.
 //
 // Layouts: activations [B][C][H][W]; conv weights [Co][Ci][3][3]; linear
 // weights [O][C].  The ReLU mask of a layer is its stored output (y > 0).

@@ -8,10 +8,14 @@ correlated with f(c), gives the unbiased estimate
 
 whose variance is var(f - g) / n instead of var(f) / n for the plain mean of
 n full multislice runs.  The surrogate here is a small convolutional network:
-input a 3 x 64 x 64 patch of the projected potential around the probe (one
-channel per third of the specimen depth, averaged over the slices of that
-third in configuration c), output the integrated detector signals at the
-readout thicknesses.  Only g's fluctuation from configuration to
+input a patch of the projected potential around the probe with one channel
+per depth bin (the mean potential of the bin's slices in configuration c; the
+workload uses one bin per readout interval, and the patch is a 64 x 64-pixel
+window around the probe averaged to 16 x 16), output the integrated detector
+signals at the readout thicknesses.  Depth-resolved inputs matter: for a weak
+phase object the phonon fluctuation of a signal is close to a linear
+functional of the potential fluctuation at each depth, with a depth-dependent
+kernel, so depth-averaged inputs lose most of it.  Only g's fluctuation from configuration to
 configuration matters, so it is trained on deviations: the patch minus its
 mean over the configurations at that position, mapped to the signal minus
 its mean.  It is trained on (patch, signal) pairs that the
@@ -25,14 +29,18 @@ import time
 
 import numpy as np
 
-CONV = ((3, 16), (16, 32), (32, 64))   # (Ci, Co) of the three 3x3 / stride-2 convolutions
+CONV = ((3, 16), (16, 32), (32, 64), (64, 64))   # (Ci, Co) of the four 3x3 / stride-2 convolutions
 PATCH = 64
 
 
 class SurrogateNet:
-    """Conv(3->16) -> Conv(16->32) -> Conv(32->64) (ReLU, stride 2) -> mean pool -> Linear(64->nout)."""
+    """Conv(cin->16) -> Conv(16->32) -> Conv(32->64) -> Conv(64->64) (stride 2, ReLU unless relu=False) ->
+    mean pool -> Linear(64->nout), on cin x size x size inputs.  On 16 x 16 inputs the last convolution
+    leaves one pixel, so the linear layer reads position-specific features of the whole patch (a mean
+    pool over a larger map would average the kernel over positions).  Without the ReLUs the network is a
+    linear map of its input with a convolutional structure."""
 
-    def __init__(self, nout: int, batch_max: int, seed: int = 0):
+    def __init__(self, nout: int, batch_max: int, seed: int = 0, cin: int = 3, size: int = PATCH, relu: bool = True):
         import torch
 
         from . import lib
@@ -40,26 +48,29 @@ class SurrogateNet:
         self.L = lib()
         self.nout = nout
         self.B = batch_max
+        self.relu = 1 if relu else 0
+        self.conv = ((cin, CONV[0][1]),) + tuple(CONV[1:])
+        self.size = size
         dev = torch.device("cuda")
         rng = np.random.default_rng(seed)
         self.params = []          # FP32 masters
         self.bf = []              # BF16 copies of conv weights
-        for (ci, co) in CONV:
+        for (ci, co) in self.conv:
             w = rng.normal(0.0, np.sqrt(2.0 / (9 * ci)), (co, ci, 3, 3)).astype(np.float32)
             self.params += [torch.from_numpy(w).to(dev), torch.zeros(co, dtype=torch.float32, device=dev)]
-        c_last = CONV[-1][1]
+        c_last = self.conv[-1][1]
         wl = rng.normal(0.0, np.sqrt(1.0 / c_last), (nout, c_last)).astype(np.float32)
         self.params += [torch.from_numpy(wl).to(dev), torch.zeros(nout, dtype=torch.float32, device=dev)]
-        self.bf = [self.params[2 * k].to(torch.bfloat16) for k in range(len(CONV))]
+        self.bf = [self.params[2 * k].to(torch.bfloat16) for k in range(len(self.conv))]
         self.m = [torch.zeros_like(p) for p in self.params]
         self.v = [torch.zeros_like(p) for p in self.params]
         self.grads = [torch.zeros_like(p) for p in self.params]
         self.step = 0
         B = batch_max
-        h = PATCH
+        h = size
         self.act = []
         self.dact = []
-        for (ci, co) in CONV:
+        for (ci, co) in self.conv:
             h //= 2
             self.act.append(torch.zeros((B, co, h, h), dtype=torch.bfloat16, device=dev))
             self.dact.append(torch.zeros((B, co, h, h), dtype=torch.float32, device=dev))
@@ -73,17 +84,17 @@ class SurrogateNet:
         return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
     def forward(self, x, B: int):
-        """x: BF16 [B, 3, 64, 64] on the device; returns out [B, nout] (a view)."""
+        """x: BF16 [B, cin, size, size] on the device; returns out [B, nout] (a view)."""
         L, s = self.L, self._stream()
         h = x
-        size = PATCH
-        for k, (ci, co) in enumerate(CONV):
+        size = self.size
+        for k, (ci, co) in enumerate(self.conv):
             e = L.JMS_NnConvForward(h.data_ptr(), self.bf[k].data_ptr(), self.params[2 * k + 1].data_ptr(),
-                                    self.act[k].data_ptr(), B, ci, size, size, co, 1, s)
+                                    self.act[k].data_ptr(), B, ci, size, size, co, self.relu, s)
             assert e == 0, e
             h = self.act[k]
             size //= 2
-        c_last = CONV[-1][1]
+        c_last = self.conv[-1][1]
         e = L.JMS_NnPoolLinearForward(h.data_ptr(), self.params[-2].data_ptr(), self.params[-1].data_ptr(),
                                       self.out.data_ptr(), B, c_last, size * size, self.nout, s)
         assert e == 0, e
@@ -96,21 +107,21 @@ class SurrogateNet:
         e = L.JMS_NnMseLoss(out.data_ptr(), t.data_ptr(), self.dout.data_ptr(), self.loss.data_ptr(),
                             B * self.nout, s)
         assert e == 0, e
-        nl = len(CONV)
-        size = PATCH >> nl
-        c_last = CONV[-1][1]
+        nl = len(self.conv)
+        size = self.size >> nl
+        c_last = self.conv[-1][1]
         e = L.JMS_NnPoolLinearBackward(self.act[-1].data_ptr(), self.params[-2].data_ptr(), self.dout.data_ptr(),
                                        self.dact[-1].data_ptr(), self.grads[-2].data_ptr(),
                                        self.grads[-1].data_ptr(), B, c_last, size * size, self.nout, s)
         assert e == 0, e
         for k in reversed(range(nl)):
-            ci, co = CONV[k]
+            ci, co = self.conv[k]
             hin = x if k == 0 else self.act[k - 1]
-            size_in = PATCH >> k
+            size_in = self.size >> k
             dx = None if k == 0 else self.dact[k - 1].data_ptr()
             e = L.JMS_NnConvBackward(hin.data_ptr(), self.bf[k].data_ptr(), self.act[k].data_ptr(),
                                      self.dact[k].data_ptr(), dx, self.grads[2 * k].data_ptr(),
-                                     self.grads[2 * k + 1].data_ptr(), B, ci, size_in, size_in, co, 1, s)
+                                     self.grads[2 * k + 1].data_ptr(), B, ci, size_in, size_in, co, self.relu, s)
             assert e == 0, e
         return self.loss
 
@@ -119,14 +130,14 @@ class SurrogateNet:
         self.step += 1
         s = self._stream()
         for k, p in enumerate(self.params):
-            pb = self.bf[k // 2].data_ptr() if (k % 2 == 0 and k // 2 < len(CONV)) else None
+            pb = self.bf[k // 2].data_ptr() if (k % 2 == 0 and k // 2 < len(self.conv)) else None
             e = self.L.JMS_NnAdam(p.data_ptr(), self.grads[k].data_ptr(), self.m[k].data_ptr(), self.v[k].data_ptr(),
                                   pb, p.numel(), lr, 0.9, 0.999, 1e-8, self.step, s)
             assert e == 0, e
         return loss
 
     def predict(self, x_all):
-        """Forward over a BF16 [n, 3, 64, 64] tensor in batches; returns a host array [n, nout]."""
+        """Forward over a BF16 [n, cin, size, size] tensor in batches; returns a host array [n, nout]."""
         import torch
 
         n = x_all.shape[0]
@@ -141,13 +152,14 @@ class SurrogateNet:
 # ---------------------------------------------------------------------------
 # inputs: potential patches of a phonon configuration
 # ---------------------------------------------------------------------------
-def channel_maps(sp, nobj: int, nslice_types: int, var: np.ndarray) -> np.ndarray:
-    """[3, ny, nx]: the mean projected potential of the slices in each third of
-    the specimen depth, in configuration var (variant index per object slice).
-    Needs the specimen's potentials (make_specimen(..., keep_potential=True))."""
+def channel_maps(sp, nobj: int, nslice_types: int, var: np.ndarray, nbins: int = 3) -> np.ndarray:
+    """[nbins, ny, nx]: the mean projected potential of the slices in each of
+    nbins equal parts of the specimen depth, in configuration var (variant
+    index per object slice).  Needs the specimen's potentials
+    (make_specimen(..., keep_potential=True))."""
     objslc = np.arange(nobj) % nslice_types
     out = []
-    for part in np.array_split(np.arange(nobj), 3):
+    for part in np.array_split(np.arange(nobj), nbins):
         acc = np.zeros(sp.potential[0].shape[1:])
         keys, counts = np.unique(np.stack([objslc[part], np.asarray(var)[part]], 1), axis=0, return_counts=True)
         for (t, v), c in zip(keys, counts):
@@ -156,15 +168,21 @@ def channel_maps(sp, nobj: int, nslice_types: int, var: np.ndarray) -> np.ndarra
     return np.stack(out)
 
 
-def patches(maps: np.ndarray, pos: np.ndarray, a: float, b: float) -> np.ndarray:
-    """[npos, 3, 64, 64] periodic patches of maps centred on the probe positions pos [npos, 2] (nm)."""
-    _, ny, nx = maps.shape
+def patches(maps: np.ndarray, pos: np.ndarray, a: float, b: float, window: int = PATCH, pool: int = 1) -> np.ndarray:
+    """[npos, C, window / pool, window / pool]: periodic window x window-pixel
+    patches of maps [C, ny, nx] centred on the probe positions pos [npos, 2]
+    (nm), averaged over pool x pool pixel blocks."""
+    c, ny, nx = maps.shape
     px = np.rint(pos[:, 0] / a * nx).astype(np.int64)
     py = np.rint(pos[:, 1] / b * ny).astype(np.int64)
-    off = np.arange(PATCH) - PATCH // 2
+    off = np.arange(window) - window // 2
     ix = (px[:, None] + off[None, :]) % nx
     iy = (py[:, None] + off[None, :]) % ny
-    return maps[:, iy[:, :, None], ix[:, None, :]].transpose(1, 0, 2, 3)
+    p = maps[:, iy[:, :, None], ix[:, None, :]].transpose(1, 0, 2, 3)
+    if pool > 1:
+        m = window // pool
+        p = p.reshape(p.shape[0], c, m, pool, m, pool).mean(axis=(3, 5))
+    return p
 
 
 def signals(J, d_pos, npos: int, var: np.ndarray, planes) -> np.ndarray:
@@ -193,8 +211,9 @@ class ControlVariate:
     pairs), so that the estimate below never has more variance than the plain
     mean in expectation: var(f - beta g) = (1 - rho^2) var(f) at the optimum."""
 
-    def __init__(self, nout: int, batch: int = 256, seed: int = 0):
-        self.net = SurrogateNet(nout, batch, seed)
+    def __init__(self, nout: int, batch: int = 256, seed: int = 0, cin: int = 3, size: int = PATCH,
+                 relu: bool = True):
+        self.net = SurrogateNet(nout, batch, seed, cin=cin, size=size, relu=relu)
         self.batch = batch
         self.xm = self.xs = None
         self.ym = self.ys = None
@@ -208,7 +227,7 @@ class ControlVariate:
 
     def fit(self, X: np.ndarray, Y: np.ndarray, Xval: np.ndarray, Yval: np.ndarray, epochs: int = 30,
             lr: float = 2e-3, seed: int = 0):
-        """X [n, 3, 64, 64] patches, Y [n, nout] signals; the epoch with the lowest
+        """X [n, cin, size, size] patches, Y [n, nout] signals; the epoch with the lowest
         loss on (Xval, Yval) is kept, and beta is fitted there.  Returns
         (training loss, validation loss) per epoch."""
         import torch
@@ -240,7 +259,7 @@ class ControlVariate:
                 best_state = [p.clone() for p in self.net.params]
         for p, q in zip(self.net.params, best_state):
             p.copy_(q)
-        for k in range(len(CONV)):
+        for k in range(len(self.net.conv)):
             self.net.bf[k].copy_(self.net.params[2 * k].to(self.net.bf[k].dtype))
         g = self.predict(Xval)
         gc, fc = g - g.mean(axis=0), Yval - Yval.mean(axis=0)
