@@ -85,6 +85,8 @@ class SurrogateNet:
 
     def forward(self, x, B: int):
         """x: BF16 [B, cin, size, size] on the device; returns out [B, nout] (a view)."""
+        if not x.is_contiguous():
+            raise ValueError("the surrogate reads its input as a C-ordered [B][C][H][W] array")
         L, s = self.L, self._stream()
         h = x
         size = self.size
@@ -141,6 +143,7 @@ class SurrogateNet:
         import torch
 
         n = x_all.shape[0]
+        x_all = x_all.contiguous()
         out = np.zeros((n, self.nout), np.float32)
         for i in range(0, n, self.B):
             b = min(self.B, n - i)
@@ -182,7 +185,7 @@ def patches(maps: np.ndarray, pos: np.ndarray, a: float, b: float, window: int =
     if pool > 1:
         m = window // pool
         p = p.reshape(p.shape[0], c, m, pool, m, pool).mean(axis=(3, 5))
-    return p
+    return np.ascontiguousarray(p)
 
 
 def signals(J, d_pos, npos: int, var: np.ndarray, planes) -> np.ndarray:
@@ -222,8 +225,10 @@ class ControlVariate:
     def _x(self, p):
         import torch
 
+        # the kernels read [n][C][H][W] in C order: a strided array must be copied
+        # into that layout first (torch.from_numpy keeps numpy's strides)
         z = (p - self.xm[None, :, None, None]) / self.xs[None, :, None, None]
-        return torch.from_numpy(z.astype(np.float32)).cuda().to(torch.bfloat16)
+        return torch.from_numpy(np.ascontiguousarray(z, dtype=np.float32)).cuda().to(torch.bfloat16).contiguous()
 
     def fit(self, X: np.ndarray, Y: np.ndarray, Xval: np.ndarray, Yval: np.ndarray, epochs: int = 30,
             lr: float = 2e-3, seed: int = 0):

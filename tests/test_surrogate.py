@@ -128,6 +128,24 @@ def test_training_fits_a_smooth_target():
     assert np.corrcoef(pred[:, 0], Y[:256, 0])[0, 1] > 0.9
 
 
+def test_patches_are_c_ordered_and_centred():
+    """The kernels read inputs as C-ordered [n][C][H][W]: patches() must return
+    that layout (a strided view fed to them reads scrambled values)."""
+    from jmultislicelib_b200 import surrogate as SG
+
+    rng = np.random.default_rng(2)
+    maps = rng.normal(size=(3, 40, 48))
+    pos = np.array([[0.25, 0.5], [1.0, 1.75]], np.float32)
+    for pool in (1, 4):
+        p = SG.patches(maps, pos, 2.0, 2.0, window=16, pool=pool)
+        assert p.flags["C_CONTIGUOUS"] and p.shape == (2, 3, 16 // pool, 16 // pool)
+    p = SG.patches(maps, pos, 2.0, 2.0, window=16)
+    px, py = int(round(0.25 / 2.0 * 48)), int(round(0.5 / 2.0 * 40))
+    assert p[0, 1, 8, 8] == maps[1, py, px]          # window centred on the probe pixel
+    q = SG.patches(maps, pos, 2.0, 2.0, window=16, pool=4)
+    np.testing.assert_allclose(q[0, 2, 0, 0], p[0, 2, :4, :4].mean())
+
+
 def test_cv_estimate_is_the_control_variate_formula():
     from jmultislicelib_b200 import surrogate as SG
 
