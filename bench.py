@@ -804,7 +804,7 @@ def run_cv(args):
     nval = max(2, len(tr_cfg) // 8)    # held-out configurations: early stopping and beta
     Xt, Yt = X[nval:].reshape(-1, *X.shape[2:]), Y[nval:].reshape(-1, nout)
     Xv, Yv = X[:nval].reshape(-1, *X.shape[2:]), Y[:nval].reshape(-1, nout)
-    cv = SG.ControlVariate(nout, batch=256, seed=1, cin=nbins, size=size, relu=not args.cv_linear)
+    cv = SG.ControlVariate(nout, batch=256, seed=1, cin=nbins, size=size, relu=args.cv_relu)
     hist, t_train = SG.timed(lambda: cv.fit(Xt, Yt, Xv, Yv, epochs=args.cv_epochs))
     # evaluation: 8x8 subset of the raster, 64 fresh configurations
     ev_pos = np.ascontiguousarray(raster.reshape(64, 64, 2)[::8, ::8].reshape(-1, 2))
@@ -838,7 +838,7 @@ def run_cv(args):
             "config": {"workload": "512^2 scan specimen, 8x8 positions, 64 phonon configurations as ground truth, "
                                    "estimator 4 full + surrogate on 64",
                        "input": f"{nbins} depth bins x {size} x {size} (64 x 64-pixel window averaged "
-                                f"{pool} x {pool})", "relu": not args.cv_linear,
+                                f"{pool} x {pool})", "relu": bool(args.cv_relu),
                        "train_configs": int(args.cv_train_configs),
                        "train_pairs": int(Xt.shape[0]), "validation_pairs": int(Xv.shape[0]),
                        "epochs": args.cv_epochs, "outputs": nout},
@@ -1413,7 +1413,8 @@ def main():
     ap.add_argument("--cv-epochs", type=int, default=30)
     ap.add_argument("--cv-bins", type=int, default=10, help="depth bins (input channels) of the surrogate")
     ap.add_argument("--cv-pool", type=int, default=4, help="pixel blocks averaged in the surrogate's input")
-    ap.add_argument("--cv-linear", action="store_true", help="surrogate convolutions without ReLU")
+    ap.add_argument("--cv-relu", action="store_true",
+                    help="surrogate convolutions with ReLU (default: a linear convolutional network)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

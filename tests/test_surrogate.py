@@ -164,7 +164,8 @@ def test_control_variate_on_a_small_scan():
     """End to end on a 128^2 specimen: signals from the library's multislice,
     depth-binned potential patches (one bin per readout interval), training on
     the library's BF16 kernels, beta fitted on held-out configurations, and the
-    variance of f - beta g on configurations the network never saw."""
+    variance of f - beta g on configurations the network never saw: the
+    trained network must remove most of the phonon variance there."""
     import torch
 
     import jmultislicelib_b200 as jb
@@ -201,12 +202,15 @@ def test_control_variate_on_a_small_scan():
     X -= X.mean(axis=0, keepdims=True)
     Y -= Y.mean(axis=0, keepdims=True)
     nout = Y.shape[-1]
-    cv = SG.ControlVariate(nout, batch=64, seed=1, cin=nbins, size=SG.PATCH // 4)
-    hist = cv.fit(X[8:32].reshape(-1, *X.shape[2:]), Y[8:32].reshape(-1, nout),
-                  X[:8].reshape(-1, *X.shape[2:]), Y[:8].reshape(-1, nout), epochs=20)
-    assert len(hist) == 20 and np.all(np.isfinite(cv.beta))
     F = Y[32:]                                   # evaluation configurations (deviations)
-    G = cv.predict(X[32:].reshape(-1, *X.shape[2:])).reshape(F.shape)
-    ratio = (F - cv.beta * G).var(axis=0).mean() / F.var(axis=0).mean()
-    print("control-variate variance ratio on the small scan:", ratio)
-    assert ratio < 1.0
+    # measured: 0.085 (linear network) and 0.24 (ReLU); a least-squares fit of
+    # the same inputs reaches 0.07
+    for relu, bar in ((False, 0.3), (True, 0.5)):
+        cv = SG.ControlVariate(nout, batch=64, seed=1, cin=nbins, size=SG.PATCH // 4, relu=relu)
+        hist = cv.fit(X[8:32].reshape(-1, *X.shape[2:]), Y[8:32].reshape(-1, nout),
+                      X[:8].reshape(-1, *X.shape[2:]), Y[:8].reshape(-1, nout), epochs=20)
+        assert len(hist) == 20 and np.all(np.isfinite(cv.beta))
+        G = cv.predict(X[32:].reshape(-1, *X.shape[2:])).reshape(F.shape)
+        ratio = (F - cv.beta * G).var(axis=0).mean() / F.var(axis=0).mean()
+        print("control-variate variance ratio on the small scan (relu %s): %.3f" % (relu, ratio))
+        assert ratio < bar, (relu, ratio)
