@@ -789,9 +789,9 @@ def run_cv(args):
     size = SG.PATCH // pool
     X, Y = [], []
     t_gen = 0.0
+    tr_patches = SG.DevicePatches(sp, cfg["nobj"], cfg["nslice_types"], tr_pos, nbins, pool=pool)
     for v in tr_cfg:
-        maps = SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v, nbins)
-        X.append(SG.patches(maps, tr_pos, sp.a, sp.b, pool=pool).astype(np.float32))
+        X.append(tr_patches(v)[0].cpu().numpy())
         y, dt = SG.timed(lambda: SG.signals(J, d_tr, len(tr_pos), v, planes))
         Y.append(y)
         t_gen += dt
@@ -817,10 +817,9 @@ def run_cv(args):
     for k, v in enumerate(ev_cfg):
         F[k], dt = SG.timed(lambda: SG.signals(J, d_ev, len(ev_pos), v, planes))
         t_full += dt
-        t0 = time.perf_counter()
-        P[k] = SG.patches(SG.channel_maps(sp, cfg["nobj"], cfg["nslice_types"], v, nbins), ev_pos, sp.a, sp.b,
-                          pool=pool)
-        t_patch += time.perf_counter() - t0
+    ev_patches = SG.DevicePatches(sp, cfg["nobj"], cfg["nslice_types"], ev_pos, nbins, pool=pool)
+    Pd, t_patch = SG.timed(lambda: ev_patches(ev_cfg))          # all 64 configurations in one launch
+    P[:] = Pd.cpu().numpy()
     P -= P.mean(axis=0, keepdims=True)
     G, t_sur = SG.timed(lambda: cv.predict(P.reshape(-1, *P.shape[2:])).reshape(F.shape))
     truth = F.mean(axis=0)
@@ -851,7 +850,7 @@ def run_cv(args):
             "loss_train_val_first_last": [hist[0], hist[-1]], "beta_mean": float(np.mean(cv.beta)),
             "seconds": {"specimen_potentials": t_spec, "training_signals": t_gen, "training": t_train,
                         "full_multislice_64": t_full, "full_multislice_4": t_full * n_few / 64,
-                        "surrogate_inference_64": t_sur, "patch_inputs_64_host": t_patch}}
+                        "surrogate_inference_64": t_sur, "patch_inputs_64_device": t_patch}}
     print(json.dumps(line))
     return 0
 

@@ -347,6 +347,17 @@ int JMS_NnMseLoss(const float* out, const float* target, float* dout, float* los
 int JMS_NnAdam(float* p, const float* g, float* m, float* v, void* p_bf16, int n, float lr, float b1, float b2,
 	float eps, int step, void* stream);
 int JMS_NnCastBf16(const float* src, void* dst, long long n, void* stream);
+/* Surrogate inputs on the device: out [nconf][npos][nbins][win/pool][win/pool]
+ * = the mean, over the object slices of each depth bin (nbins bins of
+ * nobj / nbins consecutive slices, the first nobj % nbins one slice longer)
+ * and over pool x pool pixel blocks, of the projected potential in the
+ * win x win-pixel window centred on the probe pixel (periodic).  pot [ntype]
+ * [nvar][ny][nx] float (potential of structure slice t, variant v); objslc
+ * [nobj] structure slice of each object slice; var [nconf][nobj] variant of
+ * each object slice per configuration; pix [npos][2] probe pixel (x, y).
+ * Device pointers; returns 0, 2 for bad arguments, 1 for a launch error. */
+int JMS_NnPatches(const float* pot, int ntype, int nvar, int nx, int ny, const int* objslc, int nobj, const int* var,
+	int nconf, const int* pix, int npos, int nbins, int win, int pool, float* out, void* stream);
 
 /* ---- on-device phase gratings (CJEElaSca, src/JEElaSca.h:98-273) --------
  * The 2-D projection mode of CJEElaSca::CalculatePhasegratingGPU

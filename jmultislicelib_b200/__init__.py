@@ -92,6 +92,7 @@ SIGNATURES = {
     "JMS_NnMseLoss": ([_p, _p, _p, _p, _i, _p], _i),
     "JMS_NnAdam": ([_p, _p, _p, _p, _p, _i, _f, _f, _f, _f, _i, _p], _i),
     "JMS_NnCastBf16": ([_p, _p, C.c_longlong, _p], _i),
+    "JMS_NnPatches": ([_p, _i, _i, _i, _i, _p, _i, _p, _i, _p, _i, _i, _i, _i, _p, _p], _i),
     "JMS_SliReadHeader": ([C.c_char_p, C.POINTER(JMSSliHeader)], _i),
     "JMS_SliReadData": ([C.c_char_p, _fp], _i),
     "JMS_SliWrite": ([C.c_char_p, C.POINTER(JMSSliHeader), _fp], _i),

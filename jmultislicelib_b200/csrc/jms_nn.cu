@@ -227,6 +227,43 @@ __global__ void k_cast_bf16(const float* __restrict__ s, __nv_bfloat16* __restri
 }
 
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Surrogate inputs: thread per output value out[c][p][b][u][v], the mean over
+// the object slices of depth bin b (bins of nobj / nbins slices, the first
+// nobj % nbins one slice longer) and over a pool x pool pixel block of the
+// projected potential of configuration c, in the win x win window centred on
+// pixel (px, py) of position p (periodic).
+__global__ void k_patches(const float* __restrict__ pot, int nvar, int nx, int ny, const int* __restrict__ objslc,
+	int nobj, const int* __restrict__ var, int nconf, const int* __restrict__ pix, int npos, int nbins, int win,
+	int pool, float* __restrict__ out)
+{
+	const int m = win / pool;
+	const long long n = (long long)nconf * npos * nbins * m * m;
+	const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const int v = (int)(i % m), u = (int)((i / m) % m);
+	const int b = (int)((i / ((long long)m * m)) % nbins);
+	const int p = (int)((i / ((long long)m * m * nbins)) % npos);
+	const int c = (int)(i / ((long long)m * m * nbins * npos));
+	const int q = nobj / nbins, r = nobj % nbins;
+	const int s0 = b * q + min(b, r), s1 = s0 + q + (b < r ? 1 : 0);
+	const int x0 = pix[2 * p] - win / 2 + v * pool, y0 = pix[2 * p + 1] - win / 2 + u * pool;
+	const long long N = (long long)nx * ny;
+	float acc = 0.f;
+	for (int s = s0; s < s1; s++) {
+		const float* map = pot + ((long long)objslc[s] * nvar + var[(long long)c * nobj + s]) * N;
+		for (int dy = 0; dy < pool; dy++) {
+			int y = (y0 + dy) % ny;
+			if (y < 0) y += ny;
+			for (int dx = 0; dx < pool; dx++) {
+				int x = (x0 + dx) % nx;
+				if (x < 0) x += nx;
+				acc += __ldg(map + (long long)y * nx + x);
+			}
+		}
+	}
+	out[i] = acc / (float)((s1 - s0) * pool * pool);
+}
 inline int ok(cudaStream_t) { return cudaGetLastError() == cudaSuccess ? 0 : 1; }
 
 } // namespace
@@ -298,6 +335,19 @@ int JMS_NnAdam(float* p, const float* g, float* m, float* v, void* p_bf16, int n
 	cudaStream_t s = (cudaStream_t)stream;
 	const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
 	k_adam<<<nblk(n, 256), 256, 0, s>>>(p, g, m, v, (__nv_bfloat16*)p_bf16, n, lr, b1, b2, eps, c1, c2);
+	return ok(s);
+}
+
+int JMS_NnPatches(const float* pot, int ntype, int nvar, int nx, int ny, const int* objslc, int nobj, const int* var,
+	int nconf, const int* pix, int npos, int nbins, int win, int pool, float* out, void* stream)
+{
+	if (!pot || !objslc || !var || !pix || !out || ntype < 1 || nvar < 1 || nx < 1 || ny < 1 || nobj < 1 ||
+		nconf < 1 || npos < 1 || nbins < 1 || nbins > nobj || win < 1 || pool < 1 || win % pool)
+		return 2;
+	cudaStream_t s = (cudaStream_t)stream;
+	const long long m = win / pool, n = (long long)nconf * npos * nbins * m * m;
+	k_patches<<<nblk(n, 256), 256, 0, s>>>(pot, nvar, nx, ny, objslc, nobj, var, nconf, pix, npos, nbins, win, pool,
+		out);
 	return ok(s);
 }
 

@@ -188,6 +188,45 @@ def patches(maps: np.ndarray, pos: np.ndarray, a: float, b: float, window: int =
     return np.ascontiguousarray(p)
 
 
+class DevicePatches:
+    """The inputs of channel_maps + patches computed on the device
+    (JMS_NnPatches): the specimen's potentials [ntype][nvar][ny][nx] stay on
+    the device, and each call returns the patches of a batch of
+    configurations at the probe positions."""
+
+    def __init__(self, sp, nobj: int, nslice_types: int, pos: np.ndarray, nbins: int, window: int = PATCH,
+                 pool: int = 1):
+        import torch
+
+        from . import lib
+
+        self.L = lib()
+        pot = np.stack([np.asarray(sp.potential[t], np.float32) for t in range(nslice_types)])
+        self.ntype, self.nvar, self.ny, self.nx = pot.shape
+        self.pot = torch.from_numpy(np.ascontiguousarray(pot)).cuda()
+        self.objslc = torch.from_numpy((np.arange(nobj) % nslice_types).astype(np.int32)).cuda()
+        px = np.rint(pos[:, 0] / sp.a * self.nx).astype(np.int64) % self.nx
+        py = np.rint(pos[:, 1] / sp.b * self.ny).astype(np.int64) % self.ny
+        self.pix = torch.from_numpy(np.stack([px, py], 1).astype(np.int32)).cuda()
+        self.nobj, self.npos, self.nbins, self.window, self.pool = nobj, len(pos), nbins, window, pool
+
+    def __call__(self, var: np.ndarray):
+        """var [nconf][nobj] -> device tensor [nconf][npos][nbins][m][m] (float32)."""
+        import torch
+
+        var = np.ascontiguousarray(np.atleast_2d(var), np.int32)
+        d_var = torch.from_numpy(var).cuda()
+        m = self.window // self.pool
+        out = torch.empty((var.shape[0], self.npos, self.nbins, m, m), dtype=torch.float32, device="cuda")
+        e = self.L.JMS_NnPatches(self.pot.data_ptr(), self.ntype, self.nvar, self.nx, self.ny, self.objslc.data_ptr(),
+                                 self.nobj, d_var.data_ptr(), var.shape[0], self.pix.data_ptr(), self.npos,
+                                 self.nbins, self.window, self.pool, out.data_ptr(),
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if e:
+            raise RuntimeError(f"JMS_NnPatches returned {e}")
+        return out
+
+
 def signals(J, d_pos, npos: int, var: np.ndarray, planes) -> np.ndarray:
     """Integrated detector signals [npos, len(planes) * ndet] of one phonon
     configuration var at the device positions d_pos (one multislice pass each)."""

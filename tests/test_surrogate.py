@@ -146,6 +146,25 @@ def test_patches_are_c_ordered_and_centred():
     np.testing.assert_allclose(q[0, 2, 0, 0], p[0, 2, :4, :4].mean())
 
 
+@pytest.mark.gpu
+def test_device_patches_match_host_patches():
+    """JMS_NnPatches against channel_maps + patches on a small specimen:
+    depth bins of unequal length, windows that wrap around the cell."""
+    from jmultislicelib_b200 import surrogate as SG
+    from jmultislicelib_b200 import synthetic as S
+
+    sp = S.make_specimen(96, 80, 2, 2, 2, 3, 5, 300.0, keep_potential=True)
+    nobj, nbins = 11, 3
+    rng = np.random.default_rng(4)
+    pos = np.stack([rng.uniform(0, sp.a, 7), rng.uniform(0, sp.b, 7)], 1).astype(np.float32)
+    var = rng.integers(0, 3, (5, nobj)).astype(np.int32)
+    for window, pool in ((64, 4), (32, 1)):
+        dev = SG.DevicePatches(sp, nobj, 2, pos, nbins, window=window, pool=pool)(var).cpu().numpy()
+        host = np.stack([SG.patches(SG.channel_maps(sp, nobj, 2, v, nbins), pos, sp.a, sp.b, window=window, pool=pool)
+                         for v in var])
+        np.testing.assert_allclose(dev, host, rtol=2e-5, atol=2e-6 * np.abs(host).max())
+
+
 def test_cv_estimate_is_the_control_variate_formula():
     from jmultislicelib_b200 import surrogate as SG
 
