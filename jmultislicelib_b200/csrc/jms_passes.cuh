@@ -39,6 +39,11 @@ struct RowTile {
 	static constexpr int kPartner = 1;   // lane distance of positions 2k and 2k+1
 	template <int P>
 	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid / P; pos = tid % P; }
+	// Lines of P threads (P dividing 32) lie inside one warp, and so do their
+	// exchange regions: a transform whose stages keep that role needs only
+	// warp barriers, and the warps of a CTA run their lines independently.
+	template <int P>
+	__host__ __device__ static constexpr bool warp_lines() { return 32 % P == 0; }
 	// split 1 exchange S(line, k1, j), k1 < A, j < B, rows padded to B+1
 	template <int A, int B>
 	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return (line * A + k1) * (B + 1) + j; }
@@ -92,6 +97,8 @@ struct ColTile {
 	static constexpr int PAD = (C < 16) ? C : 0;
 	template <int P>
 	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid % C; pos = tid / C; }
+	template <int P>
+	__host__ __device__ static constexpr bool warp_lines() { return false; }   // a column's positions span warps
 	template <int A, int B>
 	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return k1 * (B * C + PAD) + j * C + line; }
 	template <int A, int B>
@@ -114,15 +121,50 @@ struct ColTile {
 	static constexpr int sm3() { return 2 * R * (R * R * C + PAD); }
 };
 
+// Barrier around an exchange of lines of P threads: a warp barrier (which also
+// orders the warp's shared-memory accesses) when every line and its exchange
+// region lie inside one warp, else a CTA barrier.
+template <class Tile, int P>
+__device__ __forceinline__ void line_sync()
+{
+	if constexpr (Tile::template warp_lines<P>()) __syncwarp();
+	else __syncthreads();
+}
+
 // twiddle by table value w = exp(-2 pi i k / N) (conjugated for the inverse)
 template <bool INV>
 __device__ __forceinline__ float2 tw_mul(float2 v, float2 w) { return INV ? cmulc(v, w) : cmul(v, w); }
 
+// Stage twiddles W_N^(a b), a on the A-point side of a plan and b on the
+// B-point side: from the N-entry table in global memory (read-only path), or
+// from a CTA's shared copy laid out [a][b] with rows padded to B+1, so that
+// the lanes of a warp reading W^(k1 j) over j, or W^(n1 q2) over the pairs
+// (n1, q2 = 2m + h), fall on distinct bank pairs.
+struct TwGlobal {
+	const float2* p;
+	__device__ __forceinline__ float2 operator()(int a, int b) const { return __ldg(p + a * b); }
+};
+template <int B>
+struct TwShared {
+	const float2* s;
+	__device__ __forceinline__ float2 operator()(int a, int b) const { return s[a * (B + 1) + b]; }
+};
+// Fills a shared [A][B+1] twiddle copy from the global table; the caller
+// places a CTA barrier before its first use.
+template <int A, int B, int NT>
+__device__ __forceinline__ void fill_tw_shared(float2* tws, const float2* __restrict__ tw, int tid)
+{
+	for (int i = tid; i < A * (B + 1); i += NT) {
+		const int a = i / (B + 1), b = i - a * (B + 1);
+		tws[i] = b < B ? __ldg(tw + a * b) : make_float2(0.f, 0.f);
+	}
+}
+
 // ---- split 1 -----------------------------------------------------------------
 // in: B threads/line, thread j holds x[j + B m] (m < A)
 // out: A threads/line, thread k1 holds X[k1 + A k2] (k2 < B)
-template <int A, int B, bool INV, class Tile, int RM>
-__device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+template <int A, int B, bool INV, class Tile, int RM, class TW>
+__device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 {
 	int line, j;
 	Tile::template role<B>(tid, line, j);
@@ -130,7 +172,7 @@ __device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const fl
 	if (in_role) {
 		dft_reg<A, 1, 0, INV>(v);
 		#pragma unroll
-		for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + j * k1));
+		for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], tw(k1, j));
 		#pragma unroll
 		for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_pad<A, B>(line, k1, j)] = v[k1];
 	}
@@ -146,8 +188,8 @@ __device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const fl
 
 // in: A threads/line, thread k1 holds x[k1 + A k2] (k2 < B)
 // out: B threads/line, thread j holds y[j + B m] (m < A)
-template <int A, int B, bool INV, class Tile, int RM>
-__device__ __forceinline__ void fft_s1_inv(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+template <int A, int B, bool INV, class Tile, int RM, class TW>
+__device__ __forceinline__ void fft_s1_inv(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 {
 	// the transpose of fft_s1_fwd: per-thread B-point DFT, exchange, A-point DFT
 	fft_s1_fwd<B, A, INV, Tile>(v, sm, tw, tid);
@@ -156,18 +198,18 @@ __device__ __forceinline__ void fft_s1_inv(float2 (&v)[RM], float2* sm, const fl
 // ---- split 2 (B = 2A) ------------------------------------------------------------
 // in: B threads/line, thread j holds x[j + B m] (m < A)
 // out: B threads/line, thread (k1, h) = 2 k1 + h holds X[k1 + A (k + A h)] (k < A)
-template <int A, bool INV, class Tile, int RM>
-__device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+template <int A, bool INV, class Tile, int RM, class TW>
+__device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 {
 	constexpr int B = 2 * A;
 	int line, j;
 	Tile::template role<B>(tid, line, j);
 	dft_reg<A, 1, 0, INV>(v);
 	#pragma unroll
-	for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + j * k1));
+	for (int k1 = 1; k1 < A; k1++) v[k1] = tw_mul<INV>(v[k1], tw(k1, j));
 	#pragma unroll
 	for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_fwd<A, B>(line, k1, j)] = v[k1];
-	__syncthreads();
+	line_sync<Tile, B>();
 	const int k1 = j >> 1, h = j & 1;
 	#pragma unroll
 	for (int i = 0; i < A; i++) v[i] = sm[Tile::template s_fwd<A, B>(line, k1, 2 * i + h)];
@@ -184,13 +226,13 @@ __device__ __forceinline__ void fft_s2_fwd(float2 (&v)[RM], float2* sm, const fl
 		o.y = __shfl_xor_sync(0xffffffffu, u.y, Tile::kPartner);
 		v[k] = __ffma2_rn(make_float2(sgn, sgn), u, o);
 	});
-	__syncthreads();
+	line_sync<Tile, B>();
 }
 
 // in: B threads/line, thread (n1, h) = 2 n1 + h holds x[n1 + A (k + A h)] (k < A)
 // out: B threads/line, thread j holds y[j + B m] (m < A)
-template <int A, bool INV, class Tile, int RM>
-__device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+template <int A, bool INV, class Tile, int RM, class TW>
+__device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 {
 	constexpr int B = 2 * A;
 	int line, j;
@@ -211,14 +253,14 @@ __device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const fl
 	#pragma unroll
 	for (int m = 0; m < A; m++) {
 		const int q2 = 2 * m + h;
-		if (n1 > 0) v[m] = tw_mul<INV>(v[m], __ldg(tw + n1 * q2));
+		if (n1 > 0) v[m] = tw_mul<INV>(v[m], tw(n1, q2));
 		sm[Tile::template s_inv<A, B>(line, q2, n1)] = v[m];
 	}
-	__syncthreads();
+	line_sync<Tile, B>();
 	#pragma unroll
 	for (int i = 0; i < A; i++) v[i] = sm[Tile::template s_inv<A, B>(line, j, i)];
 	dft_reg<A, 1, 0, INV>(v);
-	__syncthreads();
+	line_sync<Tile, B>();
 }
 
 // ---- 3 stages, N = R^3 ---------------------------------------------------------
@@ -229,27 +271,27 @@ __device__ __forceinline__ void fft_s2_inv(float2 (&v)[RM], float2* sm, const fl
 //            DFT over m', twiddle W_N^(R j k2), exchange S2;
 //   stage C: thread (k1, k2 = t / R) takes the R values over j, R-point DFT.
 // S1 and S2 are separate regions, so two barriers per transform suffice.
-template <int R, bool INV, class Tile, int RM>
-__device__ __forceinline__ void fft3(float2 (&v)[RM], float2* sm, const float2* __restrict__ tw, int tid)
+template <int R, bool INV, class Tile, int RM, class TW>
+__device__ __forceinline__ void fft3(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 {
 	constexpr int T = R * R;
 	int line, t;
 	Tile::template role<T>(tid, line, t);
 	dft_reg<R, 1, 0, INV>(v);
 	#pragma unroll
-	for (int k1 = 1; k1 < R; k1++) v[k1] = tw_mul<INV>(v[k1], __ldg(tw + t * k1));
+	for (int k1 = 1; k1 < R; k1++) v[k1] = tw_mul<INV>(v[k1], tw(t, k1));
 	#pragma unroll
 	for (int k1 = 0; k1 < R; k1++) sm[Tile::template s3a<R>(line, k1, t)] = v[k1];
-	__syncthreads();
+	line_sync<Tile, T>();
 	const int k1 = t % R, jj = t / R;
 	#pragma unroll
 	for (int m = 0; m < R; m++) v[m] = sm[Tile::template s3a<R>(line, k1, jj + R * m)];
 	dft_reg<R, 1, 0, INV>(v);
 	#pragma unroll
-	for (int k2 = 1; k2 < R; k2++) v[k2] = tw_mul<INV>(v[k2], __ldg(tw + R * jj * k2));
+	for (int k2 = 1; k2 < R; k2++) v[k2] = tw_mul<INV>(v[k2], tw(R * jj, k2));
 	#pragma unroll
 	for (int k2 = 0; k2 < R; k2++) sm[Tile::template s3b<R>(line, k1, k2, jj)] = v[k2];
-	__syncthreads();
+	line_sync<Tile, T>();
 	#pragma unroll
 	for (int j = 0; j < R; j++) v[j] = sm[Tile::template s3b<R>(line, k1, jj, j)];
 	dft_reg<R, 1, 0, INV>(v);
@@ -267,24 +309,31 @@ struct Plan {
 	static constexpr int EMID = (S == 2) ? A_ : B_;                    // values per thread (middle layout)
 	static constexpr int TMAX = (T > TMID) ? T : TMID;
 	static constexpr int CC = CC_;                                     // columns per column-pass CTA
+	// the passes keep a shared [A][B+1] copy of the stage twiddles (split 2)
+	static constexpr bool SMEM_TW = (S == 2);
+	static constexpr int TWS = SMEM_TW ? A_ * (B_ + 1) : 1;
 	// line index of the e-th middle value of position pos
 	__device__ __forceinline__ static int mid(int pos, int e)
 	{
 		if constexpr (S == 2) return (pos >> 1) + A * (e + A * (pos & 1));
 		else return pos + A * e;
 	}
-	template <bool INV, class Tile>
-	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	template <bool INV, class Tile, class TW>
+	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 	{
 		if constexpr (S == 2) fft_s2_fwd<A, INV, Tile>(v, sm, tw, tid);
 		else fft_s1_fwd<A, B, INV, Tile>(v, sm, tw, tid);
 	}
-	template <bool INV, class Tile>
-	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	template <bool INV, class Tile, class TW>
+	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 	{
 		if constexpr (S == 2) fft_s2_inv<A, INV, Tile>(v, sm, tw, tid);
 		else fft_s1_inv<A, B, INV, Tile>(v, sm, tw, tid);
 	}
+	// every exchange of to_mid / from_mid takes only warp barriers (split 1
+	// changes the thread role between its stages and keeps CTA barriers)
+	template <class Tile>
+	__host__ __device__ static constexpr bool warp_local() { return S == 2 && Tile::template warp_lines<B>(); }
 	template <class Tile>
 	static constexpr int smem_elems()
 	{
@@ -305,19 +354,23 @@ struct Plan3 {
 	static constexpr int A = R_, B = R_ * R_;            // load layout: thread j holds x[j + B m], m < A
 	static constexpr int RM = R_, T = B, TMID = B, EMID = R_, TMAX = B;
 	static constexpr int CC = CC_;
+	static constexpr bool SMEM_TW = false;
+	static constexpr int TWS = 1;
 	__device__ __forceinline__ static int mid(int pos, int e) { return pos + B * e; }
-	template <bool INV, class Tile>
-	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	template <bool INV, class Tile, class TW>
+	__device__ __forceinline__ static void to_mid(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 	{
 		fft3<R_, INV, Tile>(v, sm, tw, tid);
 	}
-	template <bool INV, class Tile>
-	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const float2* tw, int tid)
+	template <bool INV, class Tile, class TW>
+	__device__ __forceinline__ static void from_mid(float2 (&v)[RM], float2* sm, const TW& tw, int tid)
 	{
 		// the second transform writes S1 before its first barrier; the barriers
 		// of the first transform already ordered all reads of S1 before it
 		fft3<R_, INV, Tile>(v, sm, tw, tid);
 	}
+	template <class Tile>
+	__host__ __device__ static constexpr bool warp_local() { return Tile::template warp_lines<B>(); }
 	template <class Tile>
 	static constexpr int smem_elems() { return Tile::template sm3<R_>(); }
 };
@@ -520,7 +573,7 @@ k_entry_rows(const PassArgs p)
 		}
 	}
 	if (p.plane >= 0 && p.ndet > 0) block_store_partials<NT>(acc, p, b);
-	PL::template to_mid<true, T>(v, sm, p.twx, tid);
+	PL::template to_mid<true, T>(v, sm, TwGlobal{p.twx}, tid);
 	int pos;
 	T::template role<PL::TMID>(tid, line, pos);
 	if (line < nval && pos < PL::TMID) {
@@ -546,6 +599,15 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 	// are all outside does nothing, and such rows are neither read nor stored
 	// (the column pass reads them as zero)
 	if (row0 > p.row_k1 && row0 + nval - 1 < p.row_k2) return;
+	__shared__ float2 tws[PL::TWS];
+	if constexpr (PL::SMEM_TW) {
+		fill_tw_shared<PL::A, PL::B, NT>(tws, p.twx, tid);
+		__syncthreads();
+	}
+	const auto tw = [&] {
+		if constexpr (PL::SMEM_TW) return TwShared<PL::B>{tws};
+		else return TwGlobal{p.twx};
+	}();
 	float2* W = p.work + (long long)b * p.wstride;
 	float2 v[PL::RM];
 	#pragma unroll
@@ -554,12 +616,16 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 	T::template role<PL::T>(tid, line, j);
 	const int yl = row0 + line;
 	const bool live = line < nval && (yl <= p.row_k1 || yl >= p.row_k2);
+	// with warp-local lines and no CTA-wide readout, a warp whose lines are
+	// all dead (band gap, past the last row) has nothing to do
+	if constexpr (!READ && PL::template warp_local<T>())
+		if (__all_sync(0xffffffffu, !live)) return;
 	if (live) {
 		const float2* src = W + (long long)yl * N;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
-	PL::template to_mid<false, T>(v, sm, p.twx, tid);
+	PL::template to_mid<false, T>(v, sm, tw, tid);
 	{
 		int pos;
 		T::template role<PL::TMID>(tid, line, pos);
@@ -597,7 +663,7 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 		}
 	}
 	if (!p.store) return;
-	PL::template from_mid<true, T>(v, sm, p.twx, tid);
+	PL::template from_mid<true, T>(v, sm, tw, tid);
 	if (live) {
 		float2* dst = W + (long long)yl * N;
 		#pragma unroll
@@ -615,9 +681,18 @@ __host__ __device__ constexpr int read_min_blocks()
 	return 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) > 0
 		? 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) : 1;
 }
+// Resident CTAs asked of the plain row pass: for plans of at most 16 values
+// a thread, the count at 64 registers (left free, the compiler took 70 at 512
+// once the warps ran their lines independently, dropping a resident CTA);
+// larger plans are left unconstrained.
+template <class PL>
+__host__ __device__ constexpr int row_min_blocks()
+{
+	return PL::RM <= 16 && 65536 / (row_lines<PL>() * PL::TMAX * 64) > 0 ? 65536 / (row_lines<PL>() * PL::TMAX * 64) : 1;
+}
 // plain row pass (READ = false); the readout planes use k_row_pass_read
 template <class PL, bool READ>
-__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
+__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, row_min_blocks<PL>())
 k_row_pass(const PassArgs p)
 {
 	row_pass_body<PL, READ>(p);
@@ -657,6 +732,12 @@ k_col_pass(const PassArgs p)
 	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
 	const int nx = NXC > 0 ? NXC : p.nx;
 	const int nval = min(C, nx - col0);
+	__shared__ float2 tws[PL::TWS];
+	if constexpr (PL::SMEM_TW) fill_tw_shared<PL::A, PL::B, C * PL::TMAX>(tws, p.twy, tid);   // barrier after the wave loads
+	const auto tw = [&] {
+		if constexpr (PL::SMEM_TW) return TwShared<PL::B>{tws};
+		else return TwGlobal{p.twy};
+	}();
 	float2* W = p.work + (long long)b * p.wstride + col0;
 	float2 v[PL::RM];
 	#pragma unroll
@@ -673,7 +754,8 @@ k_col_pass(const PassArgs p)
 		for (int m = 0; m < PL::A; m++)
 			if (lin & (1u << m)) v[m] = src[m * stride];
 	}
-	PL::template to_mid<true, T>(v, sm, p.twy, tid);
+	if constexpr (PL::SMEM_TW) __syncthreads();
+	PL::template to_mid<true, T>(v, sm, tw, tid);
 	{
 		int pos;
 		T::template role<PL::TMID>(tid, c, pos);
@@ -713,7 +795,7 @@ k_col_pass(const PassArgs p)
 			}
 		}
 	}
-	PL::template from_mid<false, T>(v, sm, p.twy, tid);
+	PL::template from_mid<false, T>(v, sm, tw, tid);
 	T::template role<PL::T>(tid, c, j);
 	if (c < nval && j < PL::T) {
 		float2* dst = W + j * nx + c;
@@ -748,7 +830,7 @@ k_exit_cols(const PassArgs p)
 			if (y <= p.in_k1 || y >= p.in_k2) v[m] = W[(long long)y * nx + c];
 		}
 	}
-	PL::template to_mid<true, T>(v, sm, p.twy, tid);
+	PL::template to_mid<true, T>(v, sm, TwGlobal{p.twy}, tid);
 	int pos;
 	T::template role<PL::TMID>(tid, c, pos);
 	if (c < nval && pos < PL::TMID) {
@@ -836,7 +918,7 @@ k_row_pass_pipe(const PassArgs p, int nlive, int rb_split, int rb_skip, int ntil
 		}
 		__syncthreads();   // the tile is in registers: bc is free for the exchanges
 		if (t + (int)gridDim.x < ntiles) prefetch(t + gridDim.x, sm + (cur ^ 1) * BUF);
-		PL::template to_mid<false, T>(v, bc, p.twx, tid);
+		PL::template to_mid<false, T>(v, bc, TwGlobal{p.twx}, tid);
 		{
 			int pos;
 			T::template role<PL::TMID>(tid, line, pos);
@@ -846,7 +928,7 @@ k_row_pass_pipe(const PassArgs p, int nlive, int rb_split, int rb_skip, int ntil
 				for (int e = 0; e < PL::EMID; e++) v[e] = cmul(v[e], __ldg(P + PL::mid(pos, e)));
 			}
 		}
-		PL::template from_mid<true, T>(v, bc, p.twx, tid);
+		PL::template from_mid<true, T>(v, bc, TwGlobal{p.twx}, tid);
 		if (live) {
 			float2* dst = p.work + (long long)b * p.wstride + (long long)yl * N;
 			#pragma unroll
@@ -903,7 +985,7 @@ k_col_pass_pipe(const PassArgs p, int ncb, int ntiles)
 		}
 		__syncthreads();
 		if (t + (int)gridDim.x < ntiles) prefetch(t + gridDim.x, sm + (cur ^ 1) * BUF);
-		PL::template to_mid<true, T>(v, bc, p.twy, tid);
+		PL::template to_mid<true, T>(v, bc, TwGlobal{p.twy}, tid);
 		{
 			int pos;
 			T::template role<PL::TMID>(tid, c, pos);
@@ -936,7 +1018,7 @@ k_col_pass_pipe(const PassArgs p, int ncb, int ntiles)
 				}
 			}
 		}
-		PL::template from_mid<false, T>(v, bc, p.twy, tid);
+		PL::template from_mid<false, T>(v, bc, TwGlobal{p.twy}, tid);
 		T::template role<PL::T>(tid, c, j);
 		if (c < nval && j < PL::T) {
 			float2* D = p.work + (long long)b * p.wstride + col0;

@@ -29,7 +29,7 @@ k_pgr_rows_inv(float2* work, long long gstride, int ny, const float2* tw)
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
-	PL::template to_mid<true, T>(v, sm, tw, tid);
+	PL::template to_mid<true, T>(v, sm, TwGlobal{tw}, tid);
 	int pos;
 	T::template role<PL::TMID>(tid, line, pos);
 	if (line < nval && pos < PL::TMID) {
@@ -71,7 +71,7 @@ k_pgr_cols(const float2* src, float2* dst, long long gstride, int nx, double c, 
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) v[m] = S[(long long)(j + PL::B * m) * nx + cc];
 	}
-	PL::template to_mid<true, T>(v, sm, tw, tid);
+	PL::template to_mid<true, T>(v, sm, TwGlobal{tw}, tid);
 	int pos;
 	T::template role<PL::TMID>(tid, cc, pos);
 	const bool act = cc < nval && pos < PL::TMID;
@@ -80,7 +80,7 @@ k_pgr_cols(const float2* src, float2* dst, long long gstride, int nx, double c, 
 		for (int e = 0; e < PL::EMID; e++) v[e] = pot_to_pgr(v[e], c);
 	}
 	if constexpr (MODE == kPgrColExpFt) {
-		PL::template from_mid<false, T>(v, sm, tw, tid);
+		PL::template from_mid<false, T>(v, sm, TwGlobal{tw}, tid);
 		T::template role<PL::T>(tid, cc, j);
 		if (cc < nval && j < PL::T) {
 			#pragma unroll
