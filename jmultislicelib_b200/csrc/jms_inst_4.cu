@@ -1,8 +1,7 @@
-// jms_inst_4.cu -- pass instantiations for plans P512b, P512c.
+// jms_inst_4.cu -- pass instantiations for plan P512b.
 #include "jms_passes.cuh"
 #include "jms_sizes.h"
 
 namespace jms {
 JMS_INSTANTIATE(P512b)
-JMS_INSTANTIATE(P512c)
 } // namespace jms

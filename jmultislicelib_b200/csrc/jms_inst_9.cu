@@ -1,8 +1,7 @@
-// jms_inst_9.cu -- pass instantiations for plans P256p, P512p (pipelined).
+// jms_inst_9.cu -- pass instantiations for plan P512c.
 #include "jms_passes.cuh"
 #include "jms_sizes.h"
 
 namespace jms {
-JMS_INSTANTIATE(P256p)
-JMS_INSTANTIATE(P512p)
+JMS_INSTANTIATE(P512c)
 } // namespace jms

@@ -24,7 +24,6 @@
 #pragma once
 #include "jms_fft.cuh"
 #include "jms_kernels.h"
-#include "jms_launch.cuh"
 #include "jms_sizes.h"
 
 namespace jms {
@@ -298,10 +297,9 @@ __device__ __forceinline__ void fft3(float2 (&v)[RM], float2* sm, const TW& tw, 
 }
 
 // ---- plans -------------------------------------------------------------------------
-template <int A_, int B_, int CC_, bool PIPE_>
+template <int A_, int B_, int CC_>
 struct Plan {
 	static constexpr int A = A_, B = B_, N = A_ * B_;
-	static constexpr bool PIPE = PIPE_;   // pipelined persistent passes (k_*_pass_pipe) without readout
 	static constexpr int S = (B_ == 2 * A_ && A_ >= 4) ? 2 : 1;
 	static constexpr int RM = (S == 2) ? A_ : (A_ > B_ ? A_ : B_);   // registers per thread (complex)
 	static constexpr int T = B_;                                       // threads per line (load layout)
@@ -350,7 +348,6 @@ struct Plan {
 template <int R_, int CC_ = 8>
 struct Plan3 {
 	static constexpr int R = R_, N = R_ * R_ * R_;
-	static constexpr bool PIPE = false;
 	static constexpr int A = R_, B = R_ * R_;            // load layout: thread j holds x[j + B m], m < A
 	static constexpr int RM = R_, T = B, TMID = B, EMID = R_, TMAX = B;
 	static constexpr int CC = CC_;
@@ -722,22 +719,17 @@ __device__ __forceinline__ unsigned live_rows(int j, int k1, int k2)
 // row stride when it is known at compile time (square grids, nx = N), so the
 // element offsets of the wave and grating accesses are constants; 0 reads it
 // from the arguments.
-template <class PL, bool READ, int NXC>
-__global__ void __launch_bounds__(PL::CC * PL::TMAX)
-k_col_pass(const PassArgs p)
+// The pass on one tile (wave b, columns col0 ... col0 + C - 1).  SYNC places a
+// CTA barrier between the wave loads and the first transform (which makes a
+// shared twiddle copy filled just before visible).
+template <class PL, bool READ, int NXC, bool SYNC, class TW>
+__device__ __forceinline__ void col_pass_tile(const PassArgs& p, int b, int col0, const TW& tw, float2* sm)
 {
 	constexpr int C = PL::CC;
 	using T = ColTile<C>;
-	extern __shared__ float2 sm[];
-	const int tid = threadIdx.x, b = blockIdx.y, col0 = blockIdx.x * C;
+	const int tid = threadIdx.x;
 	const int nx = NXC > 0 ? NXC : p.nx;
 	const int nval = min(C, nx - col0);
-	__shared__ float2 tws[PL::TWS];
-	if constexpr (PL::SMEM_TW) fill_tw_shared<PL::A, PL::B, C * PL::TMAX>(tws, p.twy, tid);   // barrier after the wave loads
-	const auto tw = [&] {
-		if constexpr (PL::SMEM_TW) return TwShared<PL::B>{tws};
-		else return TwGlobal{p.twy};
-	}();
 	float2* W = p.work + (long long)b * p.wstride + col0;
 	float2 v[PL::RM];
 	#pragma unroll
@@ -754,7 +746,7 @@ k_col_pass(const PassArgs p)
 		for (int m = 0; m < PL::A; m++)
 			if (lin & (1u << m)) v[m] = src[m * stride];
 	}
-	if constexpr (PL::SMEM_TW) __syncthreads();
+	if constexpr (SYNC) __syncthreads();
 	PL::template to_mid<true, T>(v, sm, tw, tid);
 	{
 		int pos;
@@ -806,6 +798,19 @@ k_col_pass(const PassArgs p)
 	}
 }
 
+template <class PL, bool READ, int NXC>
+__global__ void __launch_bounds__(PL::CC * PL::TMAX)
+k_col_pass(const PassArgs p)
+{
+	extern __shared__ float2 sm[];
+	__shared__ float2 tws[PL::TWS];
+	if constexpr (PL::SMEM_TW) {
+		fill_tw_shared<PL::A, PL::B, PL::CC * PL::TMAX>(tws, p.twy, threadIdx.x);   // barrier after the wave loads
+		col_pass_tile<PL, READ, NXC, true>(p, blockIdx.y, blockIdx.x * PL::CC, TwShared<PL::B>{tws}, sm);
+	}
+	else col_pass_tile<PL, READ, NXC, false>(p, blockIdx.y, blockIdx.x * PL::CC, TwGlobal{p.twy}, sm);
+}
+
 // Exit column pass: IFT_y -> real-space readout (plane), no store.
 template <class PL>
 __global__ void __launch_bounds__(PL::CC * PL::TMAX)
@@ -842,196 +847,9 @@ k_exit_cols(const PassArgs p)
 // ---------------------------------------------------------------------------
 // launchers (explicitly instantiated per size in jms_inst_*.cu)
 // ---------------------------------------------------------------------------
-// ---------------------------------------------------------------------------
-// pipelined persistent passes (no readout)
-// ---------------------------------------------------------------------------
-// A CTA walks its tiles (wave, live row block / column block) with a stride
-// of the grid size.  The lines of its next tile are copied to shared memory
-// with cp.async (16-byte chunks) while it transforms the current one, so the
-// global-load latency overlaps the transforms.  Two buffers alternate: the
-// one holding the current tile becomes the exchange space of its transforms
-// once the tile is in registers.
-__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src_gmem)
-{
-	const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src_gmem) : "memory");
-}
+// closes a group of cp.async copies (the phase-grating synthesis stages its
+// atom chunks with them)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-template <class PL, class Tile>
-__host__ __device__ constexpr int pipe_buf_elems(int tile_elems)
-{
-	return tile_elems > PL::template smem_elems<Tile>() ? tile_elems : PL::template smem_elems<Tile>();
-}
-
-// Row pass: tiles t -> wave t / nlive, live row block li = t % nlive (blocks
-// [0, rb_split) and [rb_split + rb_skip, ...): the band gap holds none).
-template <class PL>
-__global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, 3)
-k_row_pass_pipe(const PassArgs p, int nlive, int rb_split, int rb_skip, int ntiles)
-{
-	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
-	constexpr int BUF = pipe_buf_elems<PL, RowTile<L>>(L * N);
-	constexpr int CPR = N / 2;   // 16-byte chunks per row
-	using T = RowTile<L>;
-	extern __shared__ __align__(16) float2 sm[];
-	const int tid = threadIdx.x;
-	auto live_row = [&](int y) { return y <= p.row_k1 || y >= p.row_k2; };
-	auto tile = [&](int t, int& b, int& row0, int& nval) {
-		b = t / nlive;
-		const int li = t - b * nlive;
-		row0 = (li < rb_split ? li : li + rb_skip) * L;
-		nval = min(L, p.ny - row0);
-	};
-	auto prefetch = [&](int t, float2* dst) {
-		int b, row0, nval;
-		tile(t, b, row0, nval);
-		const float2* W = p.work + (long long)b * p.wstride + (long long)row0 * N;
-		#pragma unroll 1
-		for (int k = tid; k < L * CPR; k += NT) {
-			const int line = k / CPR, c = k - line * CPR;
-			if (line < nval && live_row(row0 + line)) cp_async16(dst + line * N + 2 * c, W + (long long)line * N + 2 * c);
-		}
-		cp_async_commit();
-	};
-	int cur = 0;
-	if ((int)blockIdx.x < ntiles) prefetch(blockIdx.x, sm);
-	#pragma unroll 1
-	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-		float2* bc = sm + cur * BUF;
-		int b, row0, nval;
-		tile(t, b, row0, nval);
-		cp_async_wait_all();
-		__syncthreads();
-		float2 v[PL::RM];
-		#pragma unroll
-		for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
-		int line, j;
-		T::template role<PL::T>(tid, line, j);
-		const int yl = row0 + line;
-		const bool live = line < nval && live_row(yl);
-		if (live) {
-			const float2* src = bc + line * N;
-			#pragma unroll
-			for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
-		}
-		__syncthreads();   // the tile is in registers: bc is free for the exchanges
-		if (t + (int)gridDim.x < ntiles) prefetch(t + gridDim.x, sm + (cur ^ 1) * BUF);
-		PL::template to_mid<false, T>(v, bc, TwGlobal{p.twx}, tid);
-		{
-			int pos;
-			T::template role<PL::TMID>(tid, line, pos);
-			if (line < nval && pos < PL::TMID) {
-				const float2* P = p.mul + (long long)(row0 + line) * N;
-				#pragma unroll
-				for (int e = 0; e < PL::EMID; e++) v[e] = cmul(v[e], __ldg(P + PL::mid(pos, e)));
-			}
-		}
-		PL::template from_mid<true, T>(v, bc, TwGlobal{p.twx}, tid);
-		if (live) {
-			float2* dst = p.work + (long long)b * p.wstride + (long long)yl * N;
-			#pragma unroll
-			for (int m = 0; m < PL::A; m++) dst[j + PL::B * m] = v[m];
-		}
-		cur ^= 1;
-	}
-	cp_async_wait_all();
-}
-
-// Column pass: tiles t -> wave t / ncb, column block t % ncb.
-template <class PL>
-__global__ void __launch_bounds__(PL::CC * PL::TMAX, 3)
-k_col_pass_pipe(const PassArgs p, int ncb, int ntiles)
-{
-	constexpr int C = PL::CC, N = PL::N, NT = PL::CC * PL::TMAX;
-	constexpr int BUF = pipe_buf_elems<PL, ColTile<C>>(N * C);
-	constexpr int CPR = C / 2;   // 16-byte chunks per row of the tile
-	using T = ColTile<C>;
-	extern __shared__ __align__(16) float2 sm[];
-	const int tid = threadIdx.x, nx = p.nx;
-	auto live_in = [&](int y) { return y <= p.in_k1 || y >= p.in_k2; };
-	auto prefetch = [&](int t, float2* dst) {
-		const int b = t / ncb, col0 = (t - b * ncb) * C;
-		const int nval = min(C, nx - col0);
-		const float2* W = p.work + (long long)b * p.wstride + col0;
-		#pragma unroll 1
-		for (int k = tid; k < N * CPR; k += NT) {
-			const int y = k / CPR, c2 = 2 * (k - y * CPR);
-			if (c2 < nval && live_in(y)) cp_async16(dst + y * C + c2, W + (long long)y * nx + c2);
-		}
-		cp_async_commit();
-	};
-	int cur = 0;
-	if ((int)blockIdx.x < ntiles) prefetch(blockIdx.x, sm);
-	#pragma unroll 1
-	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-		float2* bc = sm + cur * BUF;
-		const int b = t / ncb, col0 = (t - b * ncb) * C;
-		const int nval = min(C, nx - col0);
-		cp_async_wait_all();
-		__syncthreads();
-		float2 v[PL::RM];
-		#pragma unroll
-		for (int m = 0; m < PL::RM; m++) v[m] = make_float2(0.f, 0.f);
-		int c, j;
-		T::template role<PL::T>(tid, c, j);
-		if (c < nval && j < PL::T) {
-			#pragma unroll
-			for (int m = 0; m < PL::A; m++) {
-				const int y = j + PL::B * m;
-				if (live_in(y)) v[m] = bc[y * C + c];
-			}
-		}
-		__syncthreads();
-		if (t + (int)gridDim.x < ntiles) prefetch(t + gridDim.x, sm + (cur ^ 1) * BUF);
-		PL::template to_mid<true, T>(v, bc, TwGlobal{p.twy}, tid);
-		{
-			int pos;
-			T::template role<PL::TMID>(tid, c, pos);
-			if (c < nval && pos < PL::TMID) {
-				const int x = col0 + c;
-				const float2* mul = p.mul + (p.mul_w ? __ldg(p.mul_w + b) : 0);   // this wave's grating
-				if (p.npgx == nx && p.npgy == p.ny) {
-					const float2* tg = mul + x;
-					#pragma unroll
-					for (int e = 0; e < PL::EMID; e++) v[e] = cmul(v[e], __ldg(tg + (long long)PL::mid(pos, e) * nx));
-				}
-				else {
-					const int xs = x % p.npgx;
-					#pragma unroll
-					for (int e = 0; e < PL::EMID; e++)
-						v[e] = cmul(v[e], __ldg(mul + (long long)(PL::mid(pos, e) % p.npgy) * p.npgx + xs));
-				}
-				int sx = p.plas_x, sy = p.plas_y;
-				if (p.plas_w) { sx = __ldg(p.plas_w + 2 * b); sy = __ldg(p.plas_w + 2 * b + 1); }
-				if (sx | sy) {
-					const float tx = (float)(int)(((long long)sx * x) % nx) / (float)nx;
-					#pragma unroll
-					for (int e = 0; e < PL::EMID; e++) {
-						const int y = PL::mid(pos, e);
-						const float ty = (float)(int)(((long long)sy * y) % p.ny) / (float)p.ny;
-						float sn, cs;
-						sincospif(2.f * (tx + ty), &sn, &cs);
-						v[e] = cmul(v[e], make_float2(cs, sn));
-					}
-				}
-			}
-		}
-		PL::template from_mid<false, T>(v, bc, TwGlobal{p.twy}, tid);
-		T::template role<PL::T>(tid, c, j);
-		if (c < nval && j < PL::T) {
-			float2* D = p.work + (long long)b * p.wstride + col0;
-			#pragma unroll
-			for (int m = 0; m < PL::A; m++) {
-				const int y = j + PL::B * m;
-				if (y <= p.out_k1 || y >= p.out_k2) D[(long long)y * nx + c] = v[m];
-			}
-		}
-		cur ^= 1;
-	}
-	cp_async_wait_all();
-}
 
 template <class K>
 cudaError_t launch_k(K kern, dim3 grid, int threads, int smem, const PassArgs& p, cudaStream_t s)
@@ -1042,26 +860,6 @@ cudaError_t launch_k(K kern, dim3 grid, int threads, int smem, const PassArgs& p
 		if (e != cudaSuccess) return e;
 	}
 	kern<<<grid, threads, smem, s>>>(p);
-	return cudaGetLastError();
-}
-
-// Persistent launch: as many CTAs as fit on the device at once (occupancy x
-// SMs), at most one per tile.
-template <class K, class... Args>
-cudaError_t launch_pipe(K kern, int threads, int smem, long long ntiles, cudaStream_t s, Args... args)
-{
-	if (ntiles <= 0) return cudaSuccess;
-	if (smem > 48 * 1024) {
-		cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-		if (e != cudaSuccess) return e;
-	}
-	int dev = 0, nsm = 0, per_sm = 1;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-	cudaError_t e = resident_ctas(kern, threads, smem, 32, &per_sm);
-	if (e != cudaSuccess) return e;
-	const long long g = (long long)nsm * per_sm;
-	kern<<<(unsigned)(ntiles < g ? ntiles : g), threads, smem, s>>>(args...);
 	return cudaGetLastError();
 }
 
@@ -1082,23 +880,6 @@ cudaError_t launch_row_t(const PassArgs& p, cudaStream_t s)
 	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
 	const dim3 grid((p.ny + L - 1) / L, p.nwave);
 	if (p.plane >= 0) return launch_k(k_row_pass_read<PL>, grid, L * PL::TMAX, smem, p, s);
-	if constexpr (PL::PIPE) {
-		if (p.store) {
-			// live row blocks: [0, split) and [split + skip, nrb)
-			const int nrb = (p.ny + L - 1) / L;
-			int split = nrb, skip = 0;
-			if (p.row_k1 < p.ny - 1 && p.row_k2 > p.row_k1 + 1) {
-				split = p.row_k1 / L + 1;                        // blocks holding a row <= k1
-				const int first_hi = p.row_k2 / L;               // first block holding a row >= k2
-				skip = first_hi > split ? first_hi - split : 0;
-			}
-			const int nlive = nrb - skip;
-			const long long ntiles = (long long)nlive * p.nwave;
-			constexpr int smem_p = 2 * pipe_buf_elems<PL, RowTile<L>>(L * PL::N) * (int)sizeof(float2);
-			return launch_pipe(k_row_pass_pipe<PL>, L * PL::TMAX, smem_p, ntiles, s, p, nlive, split, skip,
-				(int)ntiles);
-		}
-	}
 	return launch_k(k_row_pass<PL, false>, grid, L * PL::TMAX, smem, p, s);
 }
 template <class PL>
@@ -1110,14 +891,6 @@ cudaError_t launch_col_t(const PassArgs& p, cudaStream_t s)
 	if (p.plane >= 0) {
 		if (p.nx == PL::N) return launch_k(k_col_pass<PL, true, PL::N>, grid, C * PL::TMAX, smem, p, s);
 		return launch_k(k_col_pass<PL, true, 0>, grid, C * PL::TMAX, smem, p, s);
-	}
-	if constexpr (PL::PIPE) {
-		if (p.nx % 2 == 0) {
-			const int ncb = (p.nx + C - 1) / C;
-			const long long ntiles = (long long)ncb * p.nwave;
-			constexpr int smem_p = 2 * pipe_buf_elems<PL, ColTile<C>>(PL::N * C) * (int)sizeof(float2);
-			return launch_pipe(k_col_pass_pipe<PL>, C * PL::TMAX, smem_p, ntiles, s, p, ncb, (int)ntiles);
-		}
 	}
 	if (p.nx == PL::N) return launch_k(k_col_pass<PL, false, PL::N>, grid, C * PL::TMAX, smem, p, s);
 	return launch_k(k_col_pass<PL, false, 0>, grid, C * PL::TMAX, smem, p, s);

@@ -7,7 +7,7 @@
 #include "jms_kernels.h"
 
 namespace jms {
-template <int A, int B, int CC = 16, bool PIPE = false> struct Plan;
+template <int A, int B, int CC = 16> struct Plan;
 template <int R, int CC> struct Plan3;
 
 using P16 = Plan<4, 4, 16>;
@@ -41,8 +41,6 @@ using P960 = Plan<30, 32, 16>;
 using P1024a = Plan<32, 32, 16>;
 using P1024b = Plan<32, 32, 8>;
 using P2048a = Plan<32, 64, 8>;
-using P256p = Plan<16, 16, 8, true>;    // pipelined persistent passes
-using P512p = Plan<16, 32, 8, true>;
 using P2048b = Plan<32, 64, 4>;
 
 template <class PL> int row_blocks_t(int ny);
@@ -57,10 +55,10 @@ template <class PL> cudaError_t launch_exit_t(const PassArgs& p, cudaStream_t s)
 	X(16, P16, "4x16") X(24, P24, "4x6") X(32, P32, "4x8 pair") X(40, P40, "5x8") X(48, P48, "6x8") \
 	X(64, P64a, "8x8") X(64, P64b, "4x4x4") X(80, P80, "8x10") X(96, P96, "8x12") X(120, P120, "10x12") \
 	X(128, P128a, "8x16 pair") X(128, P128b, "16x8") X(160, P160, "10x16") X(180, P180, "12x15") X(192, P192, "12x16") \
-	X(240, P240, "15x16") X(256, P256a, "16x16 c16") X(256, P256b, "16x16 c8") X(256, P256p, "16x16 c8 pipe") X(320, P320, "16x20") \
+	X(240, P240, "15x16") X(256, P256a, "16x16 c16") X(256, P256b, "16x16 c8") X(320, P320, "16x20") \
 	X(384, P384, "16x24") X(480, P480, "20x24") X(512, P512a, "16x32 pair c16") X(512, P512b, "8x8x8 c8") \
 	X(512, P512c, "16x32 pair c8") \
-	X(512, P512p, "16x32 pair c8 pipe") X(640, P640, "20x32") X(720, P720, "24x30") X(768, P768, "24x32") \
+	X(640, P640, "20x32") X(720, P720, "24x30") X(768, P768, "24x32") \
 	X(960, P960, "30x32") X(1024, P1024a, "32x32 c16") X(1024, P1024b, "32x32 c8") \
 	X(2048, P2048a, "32x64 pair c8") X(2048, P2048b, "32x64 pair c4")
 
