@@ -206,10 +206,15 @@ int JMS_ScanMultiFidelityDevice(int ctx_full, int ctx_low, int npos, const float
 		return 3;
 	if (F->Stream() == nullptr || Lo->Stream() == nullptr) return 2;
 	const size_t n = (size_t)npos * nd * ndet;
-	double* g = Lo->Scratch(2 * n);
-	if (g == nullptr) return 4;
+	// The coarse sums go to one half of the coarse context's control-variate
+	// scratch; the combine that read this half two calls ago (on the full-grid
+	// stream) must be done before the coarse stream clears it.
+	cudaEvent_t done = nullptr;
+	double* g = Lo->CvScratch(n, &done);
+	if (g == nullptr || done == nullptr) return 4;
 	double *g1 = g, *gm = g + n;
 	cudaStream_t sf = F->Stream(), sl = Lo->Stream();
+	if (cudaStreamWaitEvent(sl, done, 0) != cudaSuccess) return 5;
 	if (cudaMemsetAsync(d_out_int, 0, sizeof(double) * n, sf) != cudaSuccess) return 5;
 	if (cudaMemsetAsync(g, 0, sizeof(double) * 2 * n, sl) != cudaSuccess) return 5;
 	int e = F->ScanGPUDevice(npos, d_pos, dz, 1, varseq, d_out_int, nullptr, 0);
@@ -227,6 +232,7 @@ int JMS_ScanMultiFidelityDevice(int ctx_full, int ctx_low, int npos, const float
 		if (jms::launch_cv_combine(d_out_int, g1, gm, (long long)n, (double)(npass - 1) / (double)npass, sf) !=
 			cudaSuccess)
 			return 5;
+		if (cudaEventRecord(done, sf) != cudaSuccess) return 5;   // this half is free again after the combine
 	}
 	return 0;
 }

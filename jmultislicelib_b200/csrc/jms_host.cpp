@@ -64,6 +64,9 @@ JmsB200::~JmsB200()
 	dfree(d_shift_);
 	dfree(d_tcerr_);
 	dfree(d_scratch_);
+	dfree(d_cv_);
+	for (cudaEvent_t& e : cv_done_)
+		if (e) cudaEventDestroy(e);
 	dfree(d_mulw_);
 	dfree(d_shiftw_);
 	dfree(d_io_);
@@ -1025,6 +1028,26 @@ int JmsB200::SetPrecision(int mode)
 	if (mode > 0 && post(tc_prepare(stream_), "tensor-core tables")) return 2;
 	prec_ = mode;
 	return 0;
+}
+
+double* JmsB200::CvScratch(size_t n, cudaEvent_t* done)
+{
+	if (n > cv_cap_ || d_cv_ == nullptr) {
+		// a combine of an earlier call may run on another context's stream
+		if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+		dfree(d_cv_);
+		cv_cap_ = 0;
+		if (post(cudaMalloc(&d_cv_, sizeof(double) * 4 * n), "control-variate scratch")) return nullptr;
+		cv_cap_ = n;
+		for (cudaEvent_t& e : cv_done_) {
+			if (e) cudaEventDestroy(e);
+			e = nullptr;
+			if (post(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "control-variate scratch")) return nullptr;
+		}
+	}
+	cv_half_ ^= 1;
+	*done = cv_done_[cv_half_];
+	return d_cv_ + (size_t)cv_half_ * 2 * cv_cap_;
 }
 
 double* JmsB200::Scratch(size_t n)

@@ -178,6 +178,13 @@ public:
 	// device scratch of at least n doubles, owned by the context (grown on
 	// demand, freed with it); nullptr if the allocation fails
 	double* Scratch(size_t n);
+	// Control-variate scratch of the multi-fidelity scan on this (coarse)
+	// context: successive calls get the two halves of a 4 n buffer in turn, so
+	// a call may clear its half while the previous call's combine still reads
+	// the other one.  *done is the event to record after the combine that
+	// reads the half handed out; the call waits for its earlier record (a
+	// never-recorded event is complete) before clearing the half.
+	double* CvScratch(size_t n, cudaEvent_t* done);
 	int Status() const { return status_gpu_; }
 
 private:
@@ -254,6 +261,10 @@ private:
 	long long tc_launches_ = 0;
 	double* d_scratch_ = nullptr;
 	size_t scratch_cap_ = 0;
+	double* d_cv_ = nullptr;        // CvScratch: two halves of 2 n doubles
+	size_t cv_cap_ = 0;             // n of the current buffer
+	int cv_half_ = 0;
+	cudaEvent_t cv_done_[2] = {nullptr, nullptr};
 	int fuse_passes_ = 1;
 	int* d_mulw_ = nullptr;         // per-slice per-wave grating offsets of a fused scan launch
 	size_t mulw_cap_ = 0;

@@ -136,9 +136,13 @@ __device__ __forceinline__ float2 tw_mul(float2 v, float2 w) { return INV ? cmul
 
 // Stage twiddles W_N^(a b), a on the A-point side of a plan and b on the
 // B-point side: from the N-entry table in global memory (read-only path), or
-// from a CTA's shared copy laid out [a][b] with rows padded to B+1, so that
-// the lanes of a warp reading W^(k1 j) over j, or W^(n1 q2) over the pairs
-// (n1, q2 = 2m + h), fall on distinct bank pairs.
+// from a CTA's shared copy laid out [a][b] with rows padded to B+2.  A 64-bit
+// shared access is served per half warp, whose 16 lanes need distinct bank
+// pairs: reading W^(k1 j) over consecutive j they have them for any row
+// length, and reading W^(n1 q2) over the pairs (n1 < 8, h; q2 = 2m + h) they
+// sit at (B+2) n1 + h + 2m, distinct modulo 16 because B + 2 = 2 mod 16 for
+// B = 8, 16, 32, 64 (with rows of B+1 the lanes (n1, 1) and (n1 + 1, 0)
+// collided, doubling the wavefronts).
 struct TwGlobal {
 	const float2* p;
 	__device__ __forceinline__ float2 operator()(int a, int b) const { return __ldg(p + a * b); }
@@ -146,15 +150,15 @@ struct TwGlobal {
 template <int B>
 struct TwShared {
 	const float2* s;
-	__device__ __forceinline__ float2 operator()(int a, int b) const { return s[a * (B + 1) + b]; }
+	__device__ __forceinline__ float2 operator()(int a, int b) const { return s[a * (B + 2) + b]; }
 };
-// Fills a shared [A][B+1] twiddle copy from the global table; the caller
+// Fills a shared [A][B+2] twiddle copy from the global table; the caller
 // places a CTA barrier before its first use.
 template <int A, int B, int NT>
 __device__ __forceinline__ void fill_tw_shared(float2* tws, const float2* __restrict__ tw, int tid)
 {
-	for (int i = tid; i < A * (B + 1); i += NT) {
-		const int a = i / (B + 1), b = i - a * (B + 1);
+	for (int i = tid; i < A * (B + 2); i += NT) {
+		const int a = i / (B + 2), b = i - a * (B + 2);
 		tws[i] = b < B ? __ldg(tw + a * b) : make_float2(0.f, 0.f);
 	}
 }
@@ -307,9 +311,9 @@ struct Plan {
 	static constexpr int EMID = (S == 2) ? A_ : B_;                    // values per thread (middle layout)
 	static constexpr int TMAX = (T > TMID) ? T : TMID;
 	static constexpr int CC = CC_;                                     // columns per column-pass CTA
-	// the passes keep a shared [A][B+1] copy of the stage twiddles (split 2)
+	// the passes keep a shared [A][B+2] copy of the stage twiddles (split 2)
 	static constexpr bool SMEM_TW = (S == 2);
-	static constexpr int TWS = SMEM_TW ? A_ * (B_ + 1) : 1;
+	static constexpr int TWS = SMEM_TW ? A_ * (B_ + 2) : 1;
 	// line index of the e-th middle value of position pos
 	__device__ __forceinline__ static int mid(int pos, int e)
 	{
@@ -469,25 +473,6 @@ __device__ __forceinline__ void readout_fourier(const PassArgs& p, int b, int y,
 	readout_fourier_channels(p, b, y, kx, v);
 }
 
-// Sum of s over the CTA, stored as the partial of detector d (the warp sums
-// added in warp order, as block_store_partials does).
-template <int NT>
-__device__ __forceinline__ void block_store_partial(float s, const PassArgs& p, int b, int d)
-{
-	__shared__ float red1[NT / 32];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	s = warp_sum(s);
-	if (lane == 0) red1[warp] = s;
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		float t = 0.f;
-		#pragma unroll
-		for (int w = 0; w < NT / 32; w++) t += red1[w];
-		p.partial[(((long long)b * p.ndetslc + p.plane) * p.ndet + d) * p.nblk + blockIdx.x] = t;
-	}
-	__syncthreads();
-}
-
 // Real-space readout of psi(y, x) of wave b (ReadoutImgDet_d, src/JMultiSlice.cpp:4392-4459).
 __device__ __forceinline__ void readout_real(const PassArgs& p, int b, int y, int x, float2 v)
 {
@@ -597,10 +582,6 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 	// (the column pass reads them as zero)
 	if (row0 > p.row_k1 && row0 + nval - 1 < p.row_k2) return;
 	__shared__ float2 tws[PL::TWS];
-	if constexpr (PL::SMEM_TW) {
-		fill_tw_shared<PL::A, PL::B, NT>(tws, p.twx, tid);
-		__syncthreads();
-	}
 	const auto tw = [&] {
 		if constexpr (PL::SMEM_TW) return TwShared<PL::B>{tws};
 		else return TwGlobal{p.twx};
@@ -613,15 +594,21 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 	T::template role<PL::T>(tid, line, j);
 	const int yl = row0 + line;
 	const bool live = line < nval && (yl <= p.row_k1 || yl >= p.row_k2);
-	// with warp-local lines and no CTA-wide readout, a warp whose lines are
-	// all dead (band gap, past the last row) has nothing to do
-	if constexpr (!READ && PL::template warp_local<T>())
-		if (__all_sync(0xffffffffu, !live)) return;
 	if (live) {
 		const float2* src = W + (long long)yl * N;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) v[m] = src[j + PL::B * m];
 	}
+	// the twiddle copy is filled while the row loads are in flight, so the
+	// barrier waits for both latencies at once
+	if constexpr (PL::SMEM_TW) {
+		fill_tw_shared<PL::A, PL::B, NT>(tws, p.twx, tid);
+		__syncthreads();
+	}
+	// with warp-local lines and no CTA-wide readout, a warp whose lines are
+	// all dead (band gap, past the last row) has nothing more to do
+	if constexpr (!READ && PL::template warp_local<T>())
+		if (__all_sync(0xffffffffu, !live)) return;
 	PL::template to_mid<false, T>(v, sm, tw, tid);
 	{
 		int pos;
@@ -643,7 +630,12 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 			}
 			// integrating detectors one at a time (a rolled loop): unrolled
 			// over the detectors, the compiler kept every element's detector
-			// loads in flight (128 registers, half the plain pass's occupancy)
+			// loads in flight (128 registers, half the plain pass's occupancy).
+			// Each warp's sums wait in shared memory for one CTA barrier after
+			// the last detector; the per-warp and per-CTA summation orders are
+			// those of block_store_partials.
+			__shared__ float red[NT / 32][kMaxDet];
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 			for (int d = 0; d < p.ndet; d++) {
 				float s = 0.f;
 				if (mid_live) {
@@ -655,7 +647,17 @@ __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 						s = fmaf(cnorm(v[e]), __ldg(det + yd * p.nx + kx), s);
 					}
 				}
-				block_store_partial<NT>(s, p, b, d);
+				s = warp_sum(s);
+				if (lane == 0) red[warp][d] = s;
+			}
+			if (p.ndet > 0) {
+				__syncthreads();
+				if ((int)threadIdx.x < p.ndet) {
+					float t = 0.f;
+					#pragma unroll
+					for (int w = 0; w < NT / 32; w++) t += red[w][threadIdx.x];
+					p.partial[(((long long)b * p.ndetslc + p.plane) * p.ndet + threadIdx.x) * p.nblk + blockIdx.x] = t;
+				}
 			}
 		}
 	}

@@ -95,3 +95,35 @@ def test_multifidelity_rejects_mismatched_contexts(pair):
                                      vs.ctypes.data_as(C.POINTER(C.c_int)), out.ctypes.data_as(C.POINTER(C.c_float))) == 1
     assert J.L.JMS_ScanMultiFidelity(0, lo, len(pos), pos.ctypes.data_as(C.POINTER(C.c_float)), 0.0, 2,
                                      None, out.ctypes.data_as(C.POINTER(C.c_float))) == 1
+
+
+def test_device_calls_back_to_back(pair):
+    """Calls of JMS_ScanMultiFidelityDevice issued one after another without a
+    host synchronisation (as a scan loop issues them) give the result of a lone
+    call: each call's coarse stream waits for the full-grid stream before it
+    clears the coarse scratch that the previous call's combine reads.  Two
+    configurations make the full-grid pass the longer of the two streams, the
+    order in which an unordered clear would zero the previous call's coarse
+    sums before its combine."""
+    import ctypes as C
+
+    import torch
+
+    J, lo, pos, cfg = pair
+    pos = np.ascontiguousarray(pos, np.float32)
+    nd, ndet = J.L.GetDetetionSliceNum(), J.L.GetDetNum()
+    npass = 2
+    varseq = np.random.default_rng(5).integers(0, cfg["nvar"], (npass, cfg["nobj"])).astype(np.int32)
+    vs = varseq.ctypes.data_as(C.POINTER(C.c_int))
+    d_pos = torch.from_numpy(pos).cuda()
+    outs = [torch.zeros((len(pos), nd, ndet), dtype=torch.float64, device="cuda") for _ in range(7)]
+    torch.cuda.synchronize()
+    assert J.L.JMS_ScanMultiFidelityDevice(0, lo, len(pos), d_pos.data_ptr(), 0.0, npass, vs, outs[0].data_ptr()) == 0
+    torch.cuda.synchronize()
+    for o in outs[1:]:
+        assert J.L.JMS_ScanMultiFidelityDevice(0, lo, len(pos), d_pos.data_ptr(), 0.0, npass, vs, o.data_ptr()) == 0
+    torch.cuda.synchronize()
+    ref = outs[0].cpu().numpy()
+    assert np.abs(ref[..., 0]).max() > 0
+    for k, o in enumerate(outs[1:]):
+        assert np.array_equal(o.cpu().numpy(), ref), k
