@@ -179,14 +179,18 @@ __device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const TW
 		#pragma unroll
 		for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_pad<A, B>(line, k1, j)] = v[k1];
 	}
-	__syncthreads();
+	// with A = B both stages give a line the same threads, so a line inside a
+	// warp exchanges under a warp barrier
+	if constexpr (A == B) line_sync<Tile, B>();
+	else __syncthreads();
 	Tile::template role<A>(tid, line, j);
 	if (line < Tile::kLines && j < A) {
 		#pragma unroll
 		for (int jj = 0; jj < B; jj++) v[jj] = sm[Tile::template s_pad<A, B>(line, j, jj)];
 		dft_reg<B, 1, 0, INV>(v);
 	}
-	__syncthreads();
+	if constexpr (A == B) line_sync<Tile, B>();
+	else __syncthreads();
 }
 
 // in: A threads/line, thread k1 holds x[k1 + A k2] (k2 < B)
@@ -311,8 +315,9 @@ struct Plan {
 	static constexpr int EMID = (S == 2) ? A_ : B_;                    // values per thread (middle layout)
 	static constexpr int TMAX = (T > TMID) ? T : TMID;
 	static constexpr int CC = CC_;                                     // columns per column-pass CTA
-	// the passes keep a shared [A][B+2] copy of the stage twiddles (split 2)
-	static constexpr bool SMEM_TW = (S == 2);
+	// the passes keep a shared [A][B+2] copy of the stage twiddles (split 2,
+	// and split 1 with A = B, whose inverse indexes the table the same way)
+	static constexpr bool SMEM_TW = (S == 2 || A_ == B_);
 	static constexpr int TWS = SMEM_TW ? A_ * (B_ + 2) : 1;
 	// line index of the e-th middle value of position pos
 	__device__ __forceinline__ static int mid(int pos, int e)
@@ -333,9 +338,13 @@ struct Plan {
 		else fft_s1_inv<A, B, INV, Tile>(v, sm, tw, tid);
 	}
 	// every exchange of to_mid / from_mid takes only warp barriers (split 1
-	// changes the thread role between its stages and keeps CTA barriers)
+	// with A != B changes the thread role between its stages and keeps CTA
+	// barriers)
 	template <class Tile>
-	__host__ __device__ static constexpr bool warp_local() { return S == 2 && Tile::template warp_lines<B>(); }
+	__host__ __device__ static constexpr bool warp_local()
+	{
+		return (S == 2 || A_ == B_) && Tile::template warp_lines<B>();
+	}
 	template <class Tile>
 	static constexpr int smem_elems()
 	{
@@ -680,15 +689,18 @@ __host__ __device__ constexpr int read_min_blocks()
 	return 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) > 0
 		? 65536 / (row_lines<PL>() * PL::TMAX * (PL::RM <= 16 ? 64 : 112)) : 1;
 }
-// Resident CTAs asked of the plain row pass: for plans of at most 16 values
-// a thread, the count at 64 registers (left free, the compiler took 70 at 512
-// once the warps ran their lines independently, dropping a resident CTA);
-// larger plans are left unconstrained.
-template <class PL>
-__host__ __device__ constexpr int row_min_blocks()
+// Resident CTAs asked of a plain pass of NT threads: the count at 64
+// registers for plans of at most 16 values a thread, at 128 for larger ones.
+// Left free, the compiler took 70 (512 rows), 142 (1024 rows) and 140 (1024
+// columns) once the lines ran warp by warp and the twiddles came from shared
+// memory, each dropping a resident CTA.
+template <class PL, int NT>
+__host__ __device__ constexpr int pass_min_blocks()
 {
-	return PL::RM <= 16 && 65536 / (row_lines<PL>() * PL::TMAX * 64) > 0 ? 65536 / (row_lines<PL>() * PL::TMAX * 64) : 1;
+	return 65536 / (NT * (PL::RM <= 16 ? 64 : 128)) > 0 ? 65536 / (NT * (PL::RM <= 16 ? 64 : 128)) : 1;
 }
+template <class PL>
+__host__ __device__ constexpr int row_min_blocks() { return pass_min_blocks<PL, row_lines<PL>() * PL::TMAX>(); }
 // plain row pass (READ = false); the readout planes use k_row_pass_read
 template <class PL, bool READ>
 __global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX, row_min_blocks<PL>())
@@ -801,7 +813,7 @@ __device__ __forceinline__ void col_pass_tile(const PassArgs& p, int b, int col0
 }
 
 template <class PL, bool READ, int NXC>
-__global__ void __launch_bounds__(PL::CC * PL::TMAX)
+__global__ void __launch_bounds__(PL::CC * PL::TMAX, PL::RM > 16 && !READ ? pass_min_blocks<PL, PL::CC * PL::TMAX>() : 0)
 k_col_pass(const PassArgs p)
 {
 	extern __shared__ float2 sm[];
