@@ -180,7 +180,10 @@ int JMS_SetPassFusion(int on);
  * configurations).  Device form: d_pos [npos][2] nm and d_out_int double
  * [npos][ndetslc][ndet] on the device (d_out_int overwritten).  The two
  * contexts run concurrently on their own streams, and the call returns
- * without waiting.  d_pos must be ready for both streams.  Host form: host
+ * without waiting.  d_pos must be ready for both streams.  Successive device
+ * calls may be issued back to back: their coarse sums alternate between two
+ * halves of the coarse context's scratch, each cleared only after the combine
+ * that last read it (an event on the full context's stream).  Host form: host
  * buffers, returns after the copy back.  Returns 0, 1 (bad arguments or
  * context), 2 (a context lacks its stream / setup), 3 (the contexts' slice or
  * detector counts differ), 4 (scratch allocation), 5 (CUDA error), or an error

@@ -31,23 +31,37 @@ namespace jms {
 // ---------------------------------------------------------------------------
 // tiles: thread <-> (line, position) maps and exchange-buffer layouts
 // ---------------------------------------------------------------------------
-// Row tile: LINES rows per CTA; thread t -> (line t / P, position t % P).
-template <int LINES>
+// Row tile: LINES rows per CTA; thread t -> (line t / P, position t % P) for a
+// role of P threads per line, or (line t / W, position t % W) in every role
+// when the tile has a fixed line width W (positions P ... W - 1 then idle).
+template <int LINES, int W = 0>
 struct RowTile {
 	static constexpr int kLines = LINES;
+	static constexpr int kWidth = W;
 	static constexpr int kPartner = 1;   // lane distance of positions 2k and 2k+1
 	template <int P>
-	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid / P; pos = tid % P; }
+	__device__ __forceinline__ static void role(int tid, int& line, int& pos)
+	{
+		static_assert(W == 0 || P <= W, "a role wider than the tile's lines");
+		constexpr int Q = W > 0 ? W : P;
+		line = tid / Q;
+		pos = tid % Q;
+	}
 	// Lines of P threads (P dividing 32) lie inside one warp, and so do their
 	// exchange regions: a transform whose stages keep that role needs only
 	// warp barriers, and the warps of a CTA run their lines independently.
 	template <int P>
-	__host__ __device__ static constexpr bool warp_lines() { return 32 % P == 0; }
-	// split 1 exchange S(line, k1, j), k1 < A, j < B, rows padded to B+1
+	__host__ __device__ static constexpr bool warp_lines() { return 32 % (W > 0 ? W : P) == 0; }
+	// split 1 exchange S(line, k1, j), k1 < A, j < B, rows padded to B+1.  A
+	// line's region has the same size for <A, B> and <B, A> (the forward and
+	// inverse exchanges), so with warp-local lines one line's inverse exchange
+	// never writes into another line's forward exchange.
 	template <int A, int B>
-	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return (line * A + k1) * (B + 1) + j; }
+	__host__ __device__ static constexpr int pad_line() { return A * (B + 1) > B * (A + 1) ? A * (B + 1) : B * (A + 1); }
 	template <int A, int B>
-	static constexpr int sm_pad() { return LINES * A * (B + 1); }
+	__device__ __forceinline__ static int s_pad(int line, int k1, int j) { return line * pad_line<A, B>() + k1 * (B + 1) + j; }
+	template <int A, int B>
+	static constexpr int sm_pad() { return LINES * pad_line<A, B>(); }
 	// split 2 exchanges S(line, a, b), a < A, b < B, rows padded to B+2: the
 	// pair reads of a half warp (a = 0..7, b = 2i + h) land on 16 distinct
 	// bank pairs, and every per-thread loop has a constant address stride
@@ -94,6 +108,7 @@ struct ColTile {
 	static constexpr int kLines = C;
 	static constexpr int kPartner = C;
 	static constexpr int PAD = (C < 16) ? C : 0;
+	static constexpr int kWidth = 0;
 	template <int P>
 	__device__ __forceinline__ static void role(int tid, int& line, int& pos) { line = tid % C; pos = tid / C; }
 	template <int P>
@@ -179,9 +194,12 @@ __device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const TW
 		#pragma unroll
 		for (int k1 = 0; k1 < A; k1++) sm[Tile::template s_pad<A, B>(line, k1, j)] = v[k1];
 	}
-	// with A = B both stages give a line the same threads, so a line inside a
-	// warp exchanges under a warp barrier
-	if constexpr (A == B) line_sync<Tile, B>();
+	// with A = B, or a tile whose lines keep max(A, B) threads in every role,
+	// both stages give a line the same threads, so a line inside a warp
+	// exchanges under a warp barrier
+	constexpr int P = A > B ? A : B;
+	constexpr bool same = A == B || Tile::kWidth >= P;
+	if constexpr (same) line_sync<Tile, P>();
 	else __syncthreads();
 	Tile::template role<A>(tid, line, j);
 	if (line < Tile::kLines && j < A) {
@@ -189,7 +207,7 @@ __device__ __forceinline__ void fft_s1_fwd(float2 (&v)[RM], float2* sm, const TW
 		for (int jj = 0; jj < B; jj++) v[jj] = sm[Tile::template s_pad<A, B>(line, j, jj)];
 		dft_reg<B, 1, 0, INV>(v);
 	}
-	if constexpr (A == B) line_sync<Tile, B>();
+	if constexpr (same) line_sync<Tile, P>();
 	else __syncthreads();
 }
 
@@ -337,13 +355,19 @@ struct Plan {
 		if constexpr (S == 2) fft_s2_inv<A, INV, Tile>(v, sm, tw, tid);
 		else fft_s1_inv<A, B, INV, Tile>(v, sm, tw, tid);
 	}
-	// every exchange of to_mid / from_mid takes only warp barriers (split 1
-	// with A != B changes the thread role between its stages and keeps CTA
-	// barriers)
+	// Threads per line of the row tile in every role: a split-1 plan with
+	// B > A gives its middle role (A threads) the load role's B threads, A of
+	// them active, so a line keeps its threads through both stages; 0 (the
+	// role's own count) otherwise.  A CTA holds as many threads either way.
+	static constexpr int ROWW = (S == 1 && B_ > A_) ? B_ : 0;
+	// every exchange of to_mid / from_mid takes only warp barriers (a split-1
+	// plan with A > B changes the threads of a line between its stages and
+	// keeps CTA barriers)
 	template <class Tile>
 	__host__ __device__ static constexpr bool warp_local()
 	{
-		return (S == 2 || A_ == B_) && Tile::template warp_lines<B>();
+		if constexpr (S == 2 || A_ == B_) return Tile::template warp_lines<B>();
+		else return Tile::kWidth == B_ && B_ > A_ && Tile::template warp_lines<B>();
 	}
 	template <class Tile>
 	static constexpr int smem_elems()
@@ -364,6 +388,7 @@ struct Plan3 {
 	static constexpr int A = R_, B = R_ * R_;            // load layout: thread j holds x[j + B m], m < A
 	static constexpr int RM = R_, T = B, TMID = B, EMID = R_, TMAX = B;
 	static constexpr int CC = CC_;
+	static constexpr int ROWW = 0;
 	static constexpr bool SMEM_TW = false;
 	static constexpr int TWS = 1;
 	__device__ __forceinline__ static int mid(int pos, int e) { return pos + B * e; }
@@ -395,6 +420,9 @@ __host__ __device__ constexpr int row_lines()
 	constexpr int l = (256 / T) / m * m;
 	return l < m ? m : l;
 }
+// the row tile of a plan
+template <class PL>
+using RowTileOf = RowTile<row_lines<PL>(), PL::ROWW>;
 
 // ---------------------------------------------------------------------------
 // readouts
@@ -524,7 +552,7 @@ __global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
 k_entry_rows(const PassArgs p)
 {
 	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
-	using T = RowTile<L>;
+	using T = RowTileOf<PL>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
@@ -582,7 +610,7 @@ template <class PL, bool READ>
 __device__ __forceinline__ void row_pass_body(const PassArgs& p)
 {
 	constexpr int N = PL::N, L = row_lines<PL>(), NT = L * PL::TMAX;
-	using T = RowTile<L>;
+	using T = RowTileOf<PL>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
@@ -884,14 +912,14 @@ template <class PL>
 cudaError_t launch_entry_t(const PassArgs& p, cudaStream_t s)
 {
 	constexpr int L = row_lines<PL>();
-	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
+	constexpr int smem = PL::template smem_elems<RowTileOf<PL>>() * (int)sizeof(float2);
 	return launch_k(k_entry_rows<PL>, dim3((p.ny + L - 1) / L, p.nwave), L * PL::TMAX, smem, p, s);
 }
 template <class PL>
 cudaError_t launch_row_t(const PassArgs& p, cudaStream_t s)
 {
 	constexpr int L = row_lines<PL>();
-	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
+	constexpr int smem = PL::template smem_elems<RowTileOf<PL>>() * (int)sizeof(float2);
 	const dim3 grid((p.ny + L - 1) / L, p.nwave);
 	if (p.plane >= 0) return launch_k(k_row_pass_read<PL>, grid, L * PL::TMAX, smem, p, s);
 	return launch_k(k_row_pass<PL, false>, grid, L * PL::TMAX, smem, p, s);

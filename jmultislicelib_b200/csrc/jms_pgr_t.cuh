@@ -14,7 +14,7 @@ __global__ void __launch_bounds__(row_lines<PL>() * PL::TMAX)
 k_pgr_rows_inv(float2* work, long long gstride, int ny, const float2* tw)
 {
 	constexpr int N = PL::N, L = row_lines<PL>();
-	using T = RowTile<L>;
+	using T = RowTileOf<PL>;
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, g = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, ny - row0);
@@ -107,7 +107,7 @@ template <class PL>
 cudaError_t rows_inv_t(const PgrArgs& p, cudaStream_t s)
 {
 	constexpr int L = row_lines<PL>();
-	constexpr int smem = PL::template smem_elems<RowTile<L>>() * (int)sizeof(float2);
+	constexpr int smem = PL::template smem_elems<RowTileOf<PL>>() * (int)sizeof(float2);
 	const dim3 grid((p.ny + L - 1) / L, p.ngr);
 	cudaError_t e = smem_attr(k_pgr_rows_inv<PL>, smem);
 	if (e != cudaSuccess) return e;

@@ -99,7 +99,7 @@ def _oracle_single(J, nx, ny, nobj, ndetper, seed, ntype=1, probe_alpha=22.0, im
 @pytest.mark.parametrize("nx,ny,nobj,ndetper", [
     (256, 256, 24, 8), (512, 512, 20, 5), (384, 720, 6, 3), (1024, 1024, 4, 2), (96, 160, 10, 4),
     (240, 120, 8, 0), (480, 320, 6, 2), (768, 640, 3, 1), (960, 24, 6, 2), (16, 48, 12, 4),
-    (180, 180, 10, 4)])
+    (180, 180, 10, 4), (192, 192, 10, 4)])
 def test_sizes_match_fp64_oracle(J, nx, ny, nobj, ndetper):
     di, odi, dif, odif = _oracle_single(J, nx, ny, nobj, ndetper, seed=nx + ny)
     assert det_rel(di, odi) < TOL
