@@ -456,6 +456,8 @@ int JmsB200::InitCore(int whichcode, int)
 		weight_imgavg_ = weight_wavavg_ = 0.f;
 		dfree(d_wav0_); dfree(d_wav_); dfree(d_cppl_); dfree(d_twx_); dfree(d_twy_);
 		if (post(cudaMalloc(&d_wav0_, sizeof(float2) * n), "InitCore")) return 104;
+		wav0_k1_ = ny_ - 1;
+		wav0_k2_ = ny_;
 		if (post(cudaMalloc(&d_wav_, sizeof(float2) * n), "InitCore")) return 106;
 		if (post(cudaMalloc(&d_cppl_, sizeof(float) * n), "InitCore")) return 105;
 		cudaMemset(d_wav0_, 0, sizeof(float2) * n);
@@ -490,6 +492,26 @@ int JmsB200::SetIncidentWave(int whichcode, const float* wav, bool bTranspose)
 		const void* src = wav;
 		if (bTranspose) { transpose_into(t, (const float2*)wav, nx_, ny_); src = t.data(); }
 		if (post(cudaMemcpy(d_wav0_, src, sizeof(float2) * n, cudaMemcpyHostToDevice), "SetIncidentWave")) return 102;
+		// the longest run of all-zero rows (ky) of the incident wave: a probe
+		// inside its aperture leaves most rows zero, and the entry pass of a
+		// scan skips them (the offset phase keeps zeros zero)
+		const float* w = static_cast<const float*>(src);
+		int best0 = 0, best1 = -1, run0 = -1;
+		for (int y = 0; y <= ny_; y++) {
+			bool zero = false;
+			if (y < ny_) {
+				zero = true;
+				const float* row = w + 2 * (size_t)y * nx_;
+				for (int k = 0; k < 2 * nx_ && zero; k++) zero = (row[k] == 0.f);
+			}
+			if (zero && run0 < 0) run0 = y;
+			if (!zero && run0 >= 0) {
+				if (y - 1 - run0 > best1 - best0) { best0 = run0; best1 = y - 1; }
+				run0 = -1;
+			}
+		}
+		if (best1 >= best0) { wav0_k1_ = best0 - 1; wav0_k2_ = best1 + 1; }
+		else { wav0_k1_ = ny_ - 1; wav0_k2_ = ny_; }
 	}
 	return 0;
 }
@@ -659,6 +681,9 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 	}
 	auto plane_of = [&](int p) { return (p >= 0 && p <= nobjslc_) ? det_objslc_[p] : -1; };
 	const int islc = std::min(std::max(islc0, 0), nobjslc_);
+	// the entry skips the incident wave's zero rows when it reads that wave
+	// unshifted (no beam tilt)
+	const bool src_gap = entry_src == d_wav0_ && ibtx == 0 && ibty == 0;
 	{ // entry: [offset] -> readout at plane islc -> IFT_x
 		PassArgs p = four;
 		p.wav0 = entry_src;
@@ -667,11 +692,13 @@ int JmsB200::run_slices(int nwave, int islc0, const int* var, float weight, cons
 		p.ibtx = ibtx;
 		p.ibty = ibty;
 		p.plane = b_dif ? plane_of(islc) : -1;
+		if (src_gap) { p.row_k1 = wav0_k1_; p.row_k2 = wav0_k2_; }
 		if (post(prow_->entry(p, s), "GPUMultislice entry")) return 101;
 		launches_++;
 	}
-	// live Fourier rows (band of the propagator last applied; all after the entry)
-	int in_k1 = ny_ - 1, in_k2 = ny_;
+	// live Fourier rows (band of the propagator last applied; after the entry,
+	// the incident wave's band when the entry skipped its zero rows)
+	int in_k1 = src_gap ? wav0_k1_ : ny_ - 1, in_k2 = src_gap ? wav0_k2_ : ny_;
 	for (int j = islc; j < nobjslc_; j++) {
 		const int st = objslc_[j] % nscslc_;
 		const int ip = proidx_[st];

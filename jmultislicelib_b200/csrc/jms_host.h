@@ -215,6 +215,7 @@ private:
 	// per propagator: Fourier rows (ky, scrambled index) in (k1, k2) are zero
 	// everywhere (band limit); k1 = ny - 1 when every row has a nonzero value
 	std::vector<int> pro_k1_, pro_k2_;
+	int wav0_k1_ = 1 << 30, wav0_k2_ = 1 << 30;   // band of the incident wave's nonzero rows
 	std::vector<float> slcthick_;
 	// random numbers of the variant draws and plasmon paths
 	CRng own_rng_;

@@ -70,7 +70,8 @@ struct PassArgs {
 	// so after x P the other rows are exactly zero: the row pass skips them
 	// (row_k1/row_k2, band of its propagator), the column pass reads them as
 	// zero (in_k1/in_k2) and does not store them (out_k1/out_k2, band of the
-	// next row pass).  k1 = ny - 1 marks all rows live.
+	// next row pass).  k1 = ny - 1 marks all rows live.  For the entry pass,
+	// row_k1/row_k2 is the band of its source's live rows.
 	int row_k1 = 1 << 30, row_k2 = 1 << 30;
 	int in_k1 = 1 << 30, in_k2 = 1 << 30;
 	int out_k1 = 1 << 30, out_k2 = 1 << 30;

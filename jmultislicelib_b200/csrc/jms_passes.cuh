@@ -556,6 +556,11 @@ k_entry_rows(const PassArgs p)
 	extern __shared__ float2 sm[];
 	const int tid = threadIdx.x, b = blockIdx.y, row0 = blockIdx.x * L;
 	const int nval = min(L, p.ny - row0);
+	// Rows outside the source's band of live rows (row_k1 / row_k2: the
+	// incident wave's all-zero rows, for scans without beam tilt) are zero: a
+	// CTA of such rows does nothing, and they are neither read, read out nor
+	// stored (the first column pass reads them as zero).
+	if (row0 > p.row_k1 && row0 + nval - 1 < p.row_k2) return;
 	float2* W = p.work + (long long)b * p.wstride;
 	float2 v[PL::RM];
 	#pragma unroll
@@ -565,7 +570,7 @@ k_entry_rows(const PassArgs p)
 	for (int d = 0; d < kMaxDet; d++) acc[d] = 0.f;
 	int line, j;
 	T::template role<PL::T>(tid, line, j);
-	if (line < nval) {
+	if (line < nval && (row0 + line <= p.row_k1 || row0 + line >= p.row_k2)) {
 		const int y = row0 + line;
 		#pragma unroll
 		for (int m = 0; m < PL::A; m++) {
@@ -595,7 +600,7 @@ k_entry_rows(const PassArgs p)
 	PL::template to_mid<true, T>(v, sm, TwGlobal{p.twx}, tid);
 	int pos;
 	T::template role<PL::TMID>(tid, line, pos);
-	if (line < nval && pos < PL::TMID) {
+	if (line < nval && pos < PL::TMID && (row0 + line <= p.row_k1 || row0 + line >= p.row_k2)) {
 		float2* dst = W + (long long)(row0 + line) * N;
 		#pragma unroll
 		for (int e = 0; e < PL::EMID; e++) dst[PL::mid(pos, e)] = v[e];
