@@ -21,6 +21,12 @@
 //   split 2 (B = 2A):   the B-point stage is shared by a thread pair with a
 //       radix-2 step over warp shuffles, so every thread keeps A values in all
 //       stages: thread (k1, h) = 2 k1 + h holds X[k1 + A (k + A h)], k < A.
+// In the row passes a line whose threads fit in one warp in every stage
+// (split 2, split 1 with A = B, and split 1 with B > A on a row tile of B
+// threads per line) exchanges under warp barriers only, so the warps of a CTA
+// run their lines independently; column lines span the CTA's warps and take
+// CTA barriers.  Stage twiddles come from a shared copy (TwShared) where the
+// plan's table layout allows it.
 #pragma once
 #include "jms_fft.cuh"
 #include "jms_kernels.h"
